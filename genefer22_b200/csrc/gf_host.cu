@@ -1,0 +1,945 @@
+// gf_host.cu -- host runtime and C ABI of the B200 modular-squaring engine.
+//
+// Owns device memory, root tables, kernel plans and CUDA graphs, and
+// implements include/gfcuda.h.  The single-test calls mirror genefer's
+// `transform` interface (src/transform.h:42-256); the batch calls run many
+// tests of one size class per launch.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gfcuda.h"
+#include "gf_kernels.cuh"
+
+using namespace gfc;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+
+struct Error
+{
+	int code;
+	std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+
+#define GFC_CK(x)                                                                                     \
+	do                                                                                                \
+	{                                                                                                 \
+		const cudaError_t e_ = (x);                                                                   \
+		if (e_ != cudaSuccess) fail(GFC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
+	} while (0)
+
+inline void after_launch()
+{
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+	const cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) fail(GFC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ roots
+
+// Prime slots: set 0 = slots 0,1; set 1 = slots 2,3,4.
+const uint32_t kPrime[5] = { PrimeSet<0>::p[0], PrimeSet<0>::p[1], PrimeSet<1>::p[0], PrimeSet<1>::p[1], PrimeSet<1>::p[2] };
+
+inline uint32_t mulmod_h(uint32_t a, uint32_t b, uint32_t p) { return static_cast<uint32_t>((static_cast<uint64_t>(a) * b) % p); }
+
+uint32_t powmod_h(uint32_t a, uint64_t e, uint32_t p)
+{
+	uint32_t r = 1, y = a % p;
+	while (e != 0) { if (e & 1) r = mulmod_h(r, y, p); y = mulmod_h(y, y, p); e >>= 1; }
+	return r;
+}
+
+// Smallest generator of (Z/pZ)*: g^((p-1)/q) != 1 for every prime q | p-1.
+uint32_t primitive_root(uint32_t p)
+{
+	std::vector<uint32_t> f;
+	uint32_t m = p - 1;
+	for (uint32_t q = 2; static_cast<uint64_t>(q) * q <= m; ++q)
+		if (m % q == 0) { f.push_back(q); while (m % q == 0) m /= q; }
+	if (m > 1) f.push_back(m);
+	for (uint32_t g = 2;; ++g)
+	{
+		bool ok = true;
+		for (uint32_t q : f) if (powmod_h(g, (p - 1) / q, p) == 1) { ok = false; break; }
+		if (ok) return g;
+	}
+}
+
+inline uint32_t to_mont_h(uint32_t x, uint32_t p) { return static_cast<uint32_t>((static_cast<uint64_t>(x % p) << 32) % p); }
+
+inline uint32_t bitrev(uint32_t k, int n)
+{
+	uint32_t r = 0;
+	for (int i = 0; i < n; ++i) { r = (r << 1) | (k & 1); k >>= 1; }
+	return r;
+}
+
+// Root tables of one prime for length N = 2^n (layout described in gf_ntt.cuh):
+//   fw[k] = psi^bitrev_n(k) R,  iv[k] = psi^-bitrev_n(k) R  (k >= 1, R = 2^32),
+//   fw[0] = R^2 / N (normalisation c),  iv[0] = psi^(-N/2) c  (K).
+void build_roots(uint32_t p, int n, uint32_t *fw, uint32_t *iv)
+{
+	const uint32_t N = 1u << n;
+	const uint32_t psi = powmod_h(primitive_root(p), (p - 1) / (2ull * N), p);
+	std::vector<uint32_t> pw(N + 1);
+	pw[0] = 1;
+	for (uint32_t i = 1; i <= N; ++i) pw[i] = mulmod_h(pw[i - 1], psi, p);
+	if (pw[N] != p - 1) fail(GFC_ERR_ARG, "root table: psi is not a primitive 2N-th root");
+	for (uint32_t k = 1; k < N; ++k)
+	{
+		const uint32_t e = bitrev(k, n);
+		fw[k] = to_mont_h(pw[e], p);
+		iv[k] = to_mont_h(p - pw[N - e], p);
+	}
+	const uint32_t R1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
+	const uint32_t c = mulmod_h(mulmod_h(R1, R1, p), powmod_h(N % p, p - 2, p), p);
+	fw[0] = c;
+	iv[0] = mulmod_h(p - pw[N / 2], c, p);
+}
+
+struct DeviceTables
+{
+	int device = -1, n = 0;
+	uint32_t *d = nullptr;
+	Tables tab[2];
+	~DeviceTables()
+	{
+		if (d != nullptr) { cudaSetDevice(device); cudaFree(d); }
+	}
+};
+
+std::mutex g_tab_mu;
+std::map<std::pair<int, int>, std::weak_ptr<DeviceTables>> g_tab_cache;
+
+// Root tables for (device, n), shared by every handle of that size.
+std::shared_ptr<DeviceTables> get_tables(int device, int n)
+{
+	std::lock_guard<std::mutex> lock(g_tab_mu);
+	const auto key = std::make_pair(device, n);
+	auto it = g_tab_cache.find(key);
+	if (it != g_tab_cache.end())
+		if (auto sp = it->second.lock()) return sp;
+
+	auto t = std::make_shared<DeviceTables>();
+	t->device = device; t->n = n;
+	const size_t N = size_t(1) << n;
+	GFC_CK(cudaMalloc(&t->d, 10 * N * sizeof(uint32_t)));
+	std::vector<uint32_t> fw(N), iv(N);
+	for (int s = 0; s < 5; ++s)
+	{
+		build_roots(kPrime[s], n, fw.data(), iv.data());
+		GFC_CK(cudaMemcpy(t->d + (2 * s) * N, fw.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		GFC_CK(cudaMemcpy(t->d + (2 * s + 1) * N, iv.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+	}
+	const int slot0[2] = { 0, 2 };
+	for (int set = 0; set < 2; ++set)
+		for (int pl = 0; pl < 3; ++pl)
+		{
+			const int s = (set == 0 && pl == 2) ? 1 : slot0[set] + pl;   // set 0 has 2 planes; plane 2 unused
+			t->tab[set].fw[pl] = t->d + (2 * s) * N;
+			t->tab[set].iv[pl] = t->d + (2 * s + 1) * N;
+		}
+	g_tab_cache[key] = t;
+	return t;
+}
+
+// Exact range: with |digit| <= D = b/2 + 1 every coefficient of a product of
+// two resting registers is at most N D^2 in absolute value; the centred CRT
+// of set S is exact when N D^2 < floor(M_S / 2).
+int choose_set(uint32_t b, int n)
+{
+	const u128 D = b / 2 + 1;
+	const u128 bound = (u128(1) << n) * D * D;
+	const u128 M0 = u128(PrimeSet<0>::p[0]) * PrimeSet<0>::p[1];
+	const u128 M1 = u128(PrimeSet<1>::p[0]) * PrimeSet<1>::p[1] * PrimeSet<1>::p[2];
+	if (bound < M0 / 2) return 0;
+	if (bound < M1 / 2) return 1;
+	return -1;
+}
+
+// ------------------------------------------------------------------ launch dispatch
+
+constexpr int small_threads(int logn) { return (logn <= 12) ? (1 << (logn - 4)) : 512; }
+constexpr int ROW_THREADS = 256, COL_THREADS = 256, FIX_THREADS = 256;
+
+template <class K>
+void set_smem(K kernel, size_t smem)
+{
+	GFC_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+}
+
+// `prep` only raises the kernel's shared-memory limit (done outside graph capture).
+template <int SET, int LOGN>
+void small_t(const Args &a, int grid, cudaStream_t s, bool prep)
+{
+	constexpr int T = small_threads(LOGN);
+	constexpr size_t smem = PrimeSet<SET>::W * ((1u << LOGN) + (1u << LOGN) / 32) * 4 + T * 8;
+	if (prep) { set_smem(k_small<SET, LOGN, T>, smem); return; }
+	k_small<SET, LOGN, T><<<grid, T, smem, s>>>(a);
+	after_launch();
+}
+
+template <int SET>
+void small_set(int logn, const Args &a, int grid, cudaStream_t s, bool prep)
+{
+	switch (logn)
+	{
+		case 10: small_t<SET, 10>(a, grid, s, prep); break;
+		case 11: small_t<SET, 11>(a, grid, s, prep); break;
+		case 12: small_t<SET, 12>(a, grid, s, prep); break;
+		case 13: small_t<SET, 13>(a, grid, s, prep); break;
+		case 14: small_t<SET, 14>(a, grid, s, prep); break;
+		default: fail(GFC_ERR_ARG, "single-CTA plan needs 10 <= n <= 14");
+	}
+}
+
+void launch_small(int set, int logn, const Args &a, int grid, cudaStream_t s, bool prep)
+{
+	if (set == 0) small_set<0>(logn, a, grid, s, prep); else small_set<1>(logn, a, grid, s, prep);
+}
+
+template <int SET, int LR>
+void col_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	constexpr int R = 1 << LR, CW = col_width(LR), RS = col_stride(LR);
+	constexpr size_t smem = size_t(PrimeSet<SET>::W) * R * RS * 4;
+	if (prep) { set_smem(k_col_fwd<SET, LR>, smem); set_smem(k_col_inv<SET, LR>, smem); return; }
+	const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / CW), static_cast<unsigned>(grid_y));
+	if (inv) k_col_inv<SET, LR><<<grid, COL_THREADS, smem, s>>>(a);
+	else k_col_fwd<SET, LR><<<grid, COL_THREADS, smem, s>>>(a);
+	after_launch();
+}
+
+template <int SET>
+void col_set(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	switch (lr)
+	{
+		case 3: col_t<SET, 3>(inv, a, grid_y, s, prep); break;
+		case 4: col_t<SET, 4>(inv, a, grid_y, s, prep); break;
+		case 5: col_t<SET, 5>(inv, a, grid_y, s, prep); break;
+		case 6: col_t<SET, 6>(inv, a, grid_y, s, prep); break;
+		case 7: col_t<SET, 7>(inv, a, grid_y, s, prep); break;
+		case 8: col_t<SET, 8>(inv, a, grid_y, s, prep); break;
+		case 9: col_t<SET, 9>(inv, a, grid_y, s, prep); break;
+		case 10: col_t<SET, 10>(inv, a, grid_y, s, prep); break;
+		default: fail(GFC_ERR_ARG, "four-step plan needs 3 <= lr <= 10");
+	}
+}
+
+void launch_col(int set, int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	if (set == 0) col_set<0>(lr, inv, a, grid_y, s, prep); else col_set<1>(lr, inv, a, grid_y, s, prep);
+}
+
+template <int SET, int LC>
+void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	constexpr int C = 1 << LC;
+	constexpr size_t smem = size_t(PrimeSet<SET>::W) * (C + C / 32) * 4;
+	if (prep) { set_smem(k_row<SET, LC>, smem); return; }
+	const dim3 grid(1u << (a.n - LC), static_cast<unsigned>(grid_y));
+	k_row<SET, LC><<<grid, ROW_THREADS, smem, s>>>(a);
+	after_launch();
+}
+
+template <int SET>
+void row_set(int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	switch (lc)
+	{
+		case 8: row_t<SET, 8>(a, grid_y, s, prep); break;
+		case 9: row_t<SET, 9>(a, grid_y, s, prep); break;
+		case 10: row_t<SET, 10>(a, grid_y, s, prep); break;
+		case 11: row_t<SET, 11>(a, grid_y, s, prep); break;
+		case 12: row_t<SET, 12>(a, grid_y, s, prep); break;
+		case 13: row_t<SET, 13>(a, grid_y, s, prep); break;
+		default: fail(GFC_ERR_ARG, "four-step plan needs 8 <= n - lr <= 13");
+	}
+}
+
+void launch_row(int set, int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	if (set == 0) row_set<0>(lc, a, grid_y, s, prep); else row_set<1>(lc, a, grid_y, s, prep);
+}
+
+bool plan_valid(int n, int lr)
+{
+	if (lr == 0) return (n >= 10) && (n <= SMALL_MAX_LOGN);
+	const int lc = n - lr;
+	return (lr >= 3) && (lr <= 10) && (lc >= 8) && (lc <= 13) && (col_width(lr) <= (1 << lc));
+}
+
+int default_plan(int n)
+{
+	if (n <= SMALL_MAX_LOGN) return 0;
+	const int lc = (n >= 23) ? 13 : ((n - 3 < 12) ? n - 3 : 12);
+	return n - lc;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ batch object
+
+struct gfc_batch
+{
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	int n = 0;
+	size_t N = 0, count = 0, num_regs = 0;
+	std::vector<uint32_t> b;
+	std::vector<int> set;
+	int lr = 0;
+	std::shared_ptr<DeviceTables> tab;
+	void *mem = nullptr;
+	size_t mem_bytes = 0;
+	int32_t *regs = nullptr;
+	uint32_t *planes = nullptr, *zp = nullptr;
+	int64_t *carry = nullptr, *d_pos = nullptr;
+	TestDesc *d_desc = nullptr;
+	int32_t *d_tests = nullptr;
+	uint32_t *d_err = nullptr;
+	std::vector<TestDesc> h_desc;
+	std::vector<uint32_t *> ebits;
+	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };
+	bool capturing = false;
+
+	~gfc_batch()
+	{
+		cudaSetDevice(device);
+		for (uint32_t *e : ebits) if (e != nullptr) cudaFree(e);
+		if (mem != nullptr) cudaFree(mem);
+		if (own_stream && (stream != nullptr)) cudaStreamDestroy(stream);
+	}
+};
+
+struct gfc_graph
+{
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	~gfc_graph()
+	{
+		cudaSetDevice(device);
+		if (exec != nullptr) cudaGraphExecDestroy(exec);
+		if (graph != nullptr) cudaGraphDestroy(graph);
+	}
+};
+
+namespace {
+
+void check_reg(const gfc_batch &bt, size_t r)
+{
+	if (r >= bt.num_regs) fail(GFC_ERR_ARG, "register index out of range");
+}
+
+void check_test(const gfc_batch &bt, size_t t)
+{
+	if (t >= bt.count) fail(GFC_ERR_ARG, "test index out of range");
+}
+
+void no_capture(const gfc_batch &bt)
+{
+	if (bt.capturing) fail(GFC_ERR_STATE, "call would synchronise during graph capture");
+}
+
+Args make_args(const gfc_batch &bt, int set)
+{
+	Args a{};
+	a.desc = bt.d_desc;
+	a.tests = bt.d_tests + bt.offset[set];
+	a.pos = bt.d_pos;
+	a.err = bt.d_err;
+	a.tab = bt.tab->tab[set];
+	a.n = bt.n;
+	a.lr = bt.lr;
+	a.num_regs = static_cast<int>(bt.num_regs);
+	return a;
+}
+
+// Raises shared-memory limits of the kernels the current plan uses.
+void prepare_plan(gfc_batch &bt)
+{
+	Args a{};
+	a.n = bt.n;
+	for (int s = 0; s < 2; ++s)
+	{
+		if (bt.nset[s] == 0) continue;
+		if (bt.lr == 0) launch_small(s, bt.n, a, 0, nullptr, true);
+		else
+		{
+			launch_col(s, bt.lr, false, a, 0, nullptr, true);
+			launch_row(s, bt.n - bt.lr, a, 0, nullptr, true);
+		}
+	}
+}
+
+// Four-step squaring / product / forward transform for the tests of one set.
+void fourstep(gfc_batch &bt, int s, const Args &a)
+{
+	const int g = bt.nset[s];
+	launch_col(s, bt.lr, false, a, g, bt.stream, false);
+	launch_row(s, bt.n - bt.lr, a, g, bt.stream, false);
+	if (a.op == OP_FWD) return;
+	launch_col(s, bt.lr, true, a, g, bt.stream, false);
+	const unsigned nseg = static_cast<unsigned>(bt.N / SEG);
+	const dim3 grid((nseg + FIX_THREADS - 1) / FIX_THREADS, static_cast<unsigned>(g));
+	k_fixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
+	after_launch();
+}
+
+// count squarings of r_0 (dup_mode DUP_NONE / DUP_ALL / DUP_BITS).
+void op_square(gfc_batch &bt, int dup_mode, uint32_t count)
+{
+	if (count == 0) return;
+	for (int s = 0; s < 2; ++s)
+	{
+		if (bt.nset[s] == 0) continue;
+		Args a = make_args(bt, s);
+		a.op = OP_SQUARE; a.dup_mode = dup_mode; a.src = 0; a.dst = 0;
+		if (bt.lr == 0)
+		{
+			a.count = static_cast<int>(count);
+			launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
+		}
+		else
+		{
+			for (uint32_t j = 0; j < count; ++j)
+			{
+				a.j = (dup_mode == DUP_BITS) ? static_cast<int>(j) : 0;
+				fourstep(bt, s, a);
+			}
+		}
+	}
+	if ((bt.lr != 0) && (dup_mode == DUP_BITS))
+	{
+		const int nt = static_cast<int>(bt.count);
+		k_pos_sub<<<(nt + 255) / 256, 256, 0, bt.stream>>>(bt.d_pos, bt.d_tests, nt, static_cast<int>(count));
+		after_launch();
+	}
+}
+
+// r_m = transform(r_src) for all tests.
+void op_init_multiplicand(gfc_batch &bt, size_t src)
+{
+	check_reg(bt, src);
+	for (int s = 0; s < 2; ++s)
+	{
+		if (bt.nset[s] == 0) continue;
+		Args a = make_args(bt, s);
+		a.op = OP_FWD; a.dup_mode = DUP_NONE; a.src = static_cast<int>(src); a.dst = 0;
+		if (bt.lr == 0) launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
+		else fourstep(bt, s, a);
+	}
+}
+
+// r_dst = r_0 * r_m for all tests.
+void op_mul(gfc_batch &bt, size_t dst)
+{
+	check_reg(bt, dst);
+	for (int s = 0; s < 2; ++s)
+	{
+		if (bt.nset[s] == 0) continue;
+		Args a = make_args(bt, s);
+		a.op = OP_MUL; a.dup_mode = DUP_NONE; a.src = 0; a.dst = static_cast<int>(dst);
+		if (bt.lr == 0) launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
+		else fourstep(bt, s, a);
+	}
+}
+
+Args all_args(const gfc_batch &bt)
+{
+	Args a = make_args(bt, 0);
+	a.tests = bt.d_tests;
+	return a;
+}
+
+void op_set(gfc_batch &bt, uint32_t value)
+{
+	for (size_t i = 0; i < bt.count; ++i)
+		if (value > bt.b[i] / 2) fail(GFC_ERR_ARG, "set: value must be <= b/2");
+	Args a = all_args(bt);
+	a.dst = 0;
+	const dim3 grid(static_cast<unsigned>((bt.N + 255) / 256 < 1024 ? (bt.N + 255) / 256 : 1024), static_cast<unsigned>(bt.count));
+	k_set<<<grid, 256, 0, bt.stream>>>(a, static_cast<int32_t>(value));
+	after_launch();
+}
+
+void op_copy(gfc_batch &bt, size_t dst, size_t src)
+{
+	check_reg(bt, dst); check_reg(bt, src);
+	if (dst == src) return;
+	Args a = all_args(bt);
+	a.dst = static_cast<int>(dst); a.src = static_cast<int>(src);
+	const size_t n4 = bt.N / 4;
+	const dim3 grid(static_cast<unsigned>((n4 + 255) / 256 < 1024 ? (n4 + 255) / 256 : 1024), static_cast<unsigned>(bt.count));
+	k_copy<<<grid, 256, 0, bt.stream>>>(a);
+	after_launch();
+}
+
+int32_t *reg_ptr(gfc_batch &bt, size_t test, size_t reg) { return bt.regs + (test * bt.num_regs + reg) * bt.N; }
+
+// Waits for the stream and reports (then clears) device-side check failures.
+void op_sync(gfc_batch &bt)
+{
+	no_capture(bt);
+	GFC_CK(cudaStreamSynchronize(bt.stream));
+	uint32_t err = 0;
+	GFC_CK(cudaMemcpy(&err, bt.d_err, sizeof(err), cudaMemcpyDeviceToHost));
+	if (err != 0)
+	{
+		const uint32_t zero = 0;
+		GFC_CK(cudaMemcpy(bt.d_err, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+		fail(GFC_ERR_NUMERIC, "device check failed: a segment carry was not absorbed");
+	}
+}
+
+void check_digits(const gfc_batch &bt, size_t test, const int32_t *in)
+{
+	const int64_t lim = bt.b[test] / 2 + 1;
+	for (size_t i = 0; i < bt.N; ++i)
+		if ((in[i] > lim) || (in[i] < -lim)) fail(GFC_ERR_ARG, "digits must satisfy |d| <= b/2 + 1 (balance them first)");
+}
+
+gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_regs, int device, void *stream)
+{
+	if ((b == nullptr) || (count == 0) || (n < 10) || (n > 23) || (num_regs < 1) || (num_regs > 1024))
+		fail(GFC_ERR_ARG, "gfc_create: need b, count >= 1, 10 <= n <= 23, 1 <= num_regs <= 1024");
+	std::unique_ptr<gfc_batch> bt(new gfc_batch());
+	bt->device = device; bt->n = static_cast<int>(n); bt->N = size_t(1) << n; bt->count = count; bt->num_regs = num_regs;
+	bt->b.assign(b, b + count);
+	bt->set.resize(count);
+	for (size_t i = 0; i < count; ++i)
+	{
+		if ((b[i] < 8) || (b[i] >= (1u << 31))) fail(GFC_ERR_ARG, "base b must satisfy 8 <= b < 2^31");
+		const int s = choose_set(b[i], static_cast<int>(n));
+		if (s < 0) fail(GFC_ERR_RANGE, "(b, n) is outside the exact range of the RNS prime sets");
+		bt->set[i] = s;
+		bt->nset[s]++;
+	}
+	bt->offset[0] = 0; bt->offset[1] = bt->nset[0];
+	bt->lr = default_plan(bt->n);
+
+	GFC_CK(cudaSetDevice(device));
+	if (stream != nullptr) bt->stream = static_cast<cudaStream_t>(stream);
+	else { GFC_CK(cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking)); bt->own_stream = true; }
+	bt->tab = get_tables(device, bt->n);
+
+	const size_t N = bt->N;
+	auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+	const size_t s_regs = al(count * num_regs * N * 4), s_pl = al(count * 3 * N * 4), s_zp = s_pl;
+	const size_t s_car = al(count * (N / SEG) * 8), s_desc = al(count * sizeof(TestDesc)), s_tests = al(count * 4);
+	const size_t s_pos = al(count * 8), s_err = 256;
+	bt->mem_bytes = s_regs + s_pl + s_zp + s_car + s_desc + s_tests + s_pos + s_err;
+	GFC_CK(cudaMalloc(&bt->mem, bt->mem_bytes));
+	char *p = static_cast<char *>(bt->mem);
+	bt->regs = reinterpret_cast<int32_t *>(p); p += s_regs;
+	bt->planes = reinterpret_cast<uint32_t *>(p); p += s_pl;
+	bt->zp = reinterpret_cast<uint32_t *>(p); p += s_zp;
+	bt->carry = reinterpret_cast<int64_t *>(p); p += s_car;
+	bt->d_desc = reinterpret_cast<TestDesc *>(p); p += s_desc;
+	bt->d_tests = reinterpret_cast<int32_t *>(p); p += s_tests;
+	bt->d_pos = reinterpret_cast<int64_t *>(p); p += s_pos;
+	bt->d_err = reinterpret_cast<uint32_t *>(p);
+	GFC_CK(cudaMemsetAsync(bt->mem, 0, bt->mem_bytes, bt->stream));
+
+	bt->h_desc.resize(count);
+	bt->ebits.assign(count, nullptr);
+	std::vector<int32_t> tests;
+	for (int s = 0; s < 2; ++s)
+		for (size_t i = 0; i < count; ++i)
+			if (bt->set[i] == s) tests.push_back(static_cast<int32_t>(i));
+	for (size_t i = 0; i < count; ++i)
+	{
+		TestDesc &d = bt->h_desc[i];
+		d.regs = bt->regs + i * num_regs * N;
+		d.planes = bt->planes + i * 3 * N;
+		d.zp = bt->zp + i * 3 * N;
+		d.carry = bt->carry + i * (N / SEG);
+		d.ebits = nullptr;
+		d.b = b[i];
+		d.binv = ~uint64_t(0) / b[i];
+		d.set = bt->set[i];
+	}
+	GFC_CK(cudaMemcpyAsync(bt->d_desc, bt->h_desc.data(), count * sizeof(TestDesc), cudaMemcpyHostToDevice, bt->stream));
+	GFC_CK(cudaMemcpyAsync(bt->d_tests, tests.data(), count * sizeof(int32_t), cudaMemcpyHostToDevice, bt->stream));
+	std::vector<int64_t> pos(count, -1);
+	GFC_CK(cudaMemcpyAsync(bt->d_pos, pos.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, bt->stream));
+	GFC_CK(cudaStreamSynchronize(bt->stream));
+	prepare_plan(*bt);
+	return bt.release();
+}
+
+template <class F>
+int guard(F &&f)
+{
+	try
+	{
+		f();
+		return GFC_OK;
+	}
+	catch (const Error &e)
+	{
+		g_err = e.msg;
+		return e.code;
+	}
+	catch (const std::exception &e)
+	{
+		g_err = e.what();
+		return GFC_ERR_CUDA;
+	}
+}
+
+#define GFC_NULLCHK(p) \
+	if ((p) == nullptr) fail(GFC_ERR_ARG, "null handle or pointer")
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+#define GFC_API extern "C" __attribute__((visibility("default")))
+
+GFC_API const char *gfc_last_error(void) { return g_err.c_str(); }
+GFC_API int gfc_version(void) { return 100; }
+GFC_API uint64_t gfc_launch_count(void) { return g_launches.load(); }
+
+// ---- single test
+
+GFC_API int gfc_create(uint32_t b, uint32_t n, size_t num_regs, int device, void *stream, gfc_transform **out)
+{
+	return guard([&] {
+		GFC_NULLCHK(out);
+		*out = nullptr;
+		*out = batch_create(&b, 1, n, num_regs, device, stream);
+	});
+}
+
+GFC_API void gfc_destroy(gfc_transform *t) { delete t; }
+
+GFC_API int gfc_set(gfc_transform *t, uint32_t a)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_set(*t, a); });
+}
+
+GFC_API int gfc_square_dup(gfc_transform *t, int dup)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_square(*t, dup ? DUP_ALL : DUP_NONE, 1); });
+}
+
+GFC_API int gfc_init_multiplicand(gfc_transform *t, size_t src)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_init_multiplicand(*t, src); });
+}
+
+GFC_API int gfc_mul(gfc_transform *t)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_mul(*t, 0); });
+}
+
+GFC_API int gfc_copy(gfc_transform *t, size_t dst, size_t src)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_copy(*t, dst, src); });
+}
+
+GFC_API int gfc_get_zi(gfc_transform *t, int32_t *zi)
+{
+	return gfc_batch_get_zi(t, 0, 0, zi);
+}
+
+GFC_API int gfc_set_zi(gfc_transform *t, const int32_t *zi)
+{
+	return gfc_batch_set_zi(t, 0, 0, zi);
+}
+
+GFC_API size_t gfc_get_mem_size(const gfc_transform *t) { return (t == nullptr) ? 0 : t->mem_bytes; }
+
+GFC_API size_t gfc_get_cache_size(const gfc_transform *t)
+{
+	if (t == nullptr) return 0;
+	return (t->set[0] == 0 ? 2 : 3) * t->N * sizeof(uint32_t) + t->N * sizeof(int32_t);
+}
+
+GFC_API size_t gfc_context_size(const gfc_transform *t, size_t num_regs)
+{
+	return (t == nullptr) ? 0 : sizeof(uint32_t) + num_regs * t->N * sizeof(int32_t);
+}
+
+GFC_API int gfc_save_context(gfc_transform *t, void *buf, size_t size, size_t num_regs)
+{
+	return guard([&] {
+		GFC_NULLCHK(t); GFC_NULLCHK(buf);
+		if ((num_regs == 0) || (num_regs > t->num_regs) || (size < gfc_context_size(t, num_regs)))
+			fail(GFC_ERR_ARG, "save_context: bad register count or buffer size");
+		no_capture(*t);
+		cudaSetDevice(t->device);
+		const uint32_t kind = GFC_CONTEXT_KIND;
+		std::memcpy(buf, &kind, sizeof(kind));
+		GFC_CK(cudaMemcpyAsync(static_cast<char *>(buf) + sizeof(kind), t->regs, num_regs * t->N * sizeof(int32_t),
+							   cudaMemcpyDeviceToHost, t->stream));
+		op_sync(*t);
+	});
+}
+
+GFC_API int gfc_read_context(gfc_transform *t, const void *buf, size_t size, size_t num_regs)
+{
+	return guard([&] {
+		GFC_NULLCHK(t); GFC_NULLCHK(buf);
+		if ((num_regs == 0) || (num_regs > t->num_regs)) fail(GFC_ERR_ARG, "read_context: bad register count");
+		uint32_t kind = 0;
+		if (size >= sizeof(kind)) std::memcpy(&kind, buf, sizeof(kind));
+		if ((kind != GFC_CONTEXT_KIND) || (size != gfc_context_size(t, num_regs)))
+			fail(GFC_ERR_STATE, "read_context: context kind or size mismatch");
+		const int32_t *d = reinterpret_cast<const int32_t *>(static_cast<const char *>(buf) + sizeof(kind));
+		for (size_t r = 0; r < num_regs; ++r) check_digits(*t, 0, d + r * t->N);
+		no_capture(*t);
+		cudaSetDevice(t->device);
+		GFC_CK(cudaMemcpyAsync(t->regs, d, num_regs * t->N * sizeof(int32_t), cudaMemcpyHostToDevice, t->stream));
+		op_sync(*t);
+	});
+}
+
+GFC_API int gfc_width(const gfc_transform *t) { return (t == nullptr) ? GFC_ERR_ARG : (t->set[0] == 0 ? 2 : 3); }
+
+GFC_API int gfc_sync(gfc_transform *t)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_sync(*t); });
+}
+
+// ---- batches
+
+GFC_API int gfc_batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_regs, int device, void *stream,
+							 gfc_batch **out)
+{
+	return guard([&] {
+		GFC_NULLCHK(out);
+		*out = nullptr;
+		*out = batch_create(b, count, n, num_regs, device, stream);
+	});
+}
+
+GFC_API void gfc_batch_destroy(gfc_batch *bt) { delete bt; }
+GFC_API size_t gfc_batch_count(const gfc_batch *bt) { return (bt == nullptr) ? 0 : bt->count; }
+
+GFC_API int gfc_batch_set(gfc_batch *bt, uint32_t a)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_set(*bt, a); });
+}
+
+GFC_API int gfc_batch_copy(gfc_batch *bt, size_t dst, size_t src)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_copy(*bt, dst, src); });
+}
+
+GFC_API int gfc_batch_square(gfc_batch *bt, int dup, uint32_t count)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_square(*bt, dup ? DUP_ALL : DUP_NONE, count); });
+}
+
+GFC_API int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *words, uint64_t nbits)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(words);
+		check_test(*bt, test);
+		no_capture(*bt);
+		if (nbits == 0) fail(GFC_ERR_ARG, "set_exponent: empty exponent");
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+		const size_t nw = (nbits + 31) / 32;
+		if (bt->ebits[test] != nullptr) { GFC_CK(cudaFree(bt->ebits[test])); bt->ebits[test] = nullptr; }
+		GFC_CK(cudaMalloc(&bt->ebits[test], nw * sizeof(uint32_t)));
+		GFC_CK(cudaMemcpy(bt->ebits[test], words, nw * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		bt->h_desc[test].ebits = bt->ebits[test];
+		GFC_CK(cudaMemcpy(bt->d_desc + test, &bt->h_desc[test], sizeof(TestDesc), cudaMemcpyHostToDevice));
+		const int64_t pos = static_cast<int64_t>(nbits) - 1;
+		GFC_CK(cudaMemcpy(bt->d_pos + test, &pos, sizeof(pos), cudaMemcpyHostToDevice));
+	});
+}
+
+GFC_API int gfc_batch_set_pos(gfc_batch *bt, const int64_t *pos)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(pos);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		for (size_t i = 0; i < bt->count; ++i)
+			if ((pos[i] >= 0) && (bt->ebits[i] == nullptr)) fail(GFC_ERR_STATE, "set_pos: test has no exponent");
+		GFC_CK(cudaMemcpyAsync(bt->d_pos, pos, bt->count * sizeof(int64_t), cudaMemcpyHostToDevice, bt->stream));
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+	});
+}
+
+GFC_API int gfc_batch_get_pos(gfc_batch *bt, int64_t *pos)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(pos);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaMemcpyAsync(pos, bt->d_pos, bt->count * sizeof(int64_t), cudaMemcpyDeviceToHost, bt->stream));
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+	});
+}
+
+GFC_API int gfc_batch_square_exp(gfc_batch *bt, uint32_t count)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt);
+		cudaSetDevice(bt->device);
+		op_square(*bt, DUP_BITS, count);
+	});
+}
+
+GFC_API int gfc_batch_init_multiplicand(gfc_batch *bt, size_t src)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_init_multiplicand(*bt, src); });
+}
+
+GFC_API int gfc_batch_mul(gfc_batch *bt, size_t dst)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_mul(*bt, dst); });
+}
+
+GFC_API int gfc_batch_gl_step(gfc_batch *bt)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt);
+		if (bt->num_regs < 2) fail(GFC_ERR_STATE, "gl_step needs 2 registers");
+		cudaSetDevice(bt->device);
+		op_init_multiplicand(*bt, 1);
+		op_mul(*bt, 1);
+	});
+}
+
+GFC_API int gfc_batch_get_zi(gfc_batch *bt, size_t test, size_t reg, int32_t *out)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(out);
+		check_test(*bt, test); check_reg(*bt, reg);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaMemcpyAsync(out, reg_ptr(*bt, test, reg), bt->N * sizeof(int32_t), cudaMemcpyDeviceToHost, bt->stream));
+		op_sync(*bt);
+	});
+}
+
+GFC_API int gfc_batch_set_zi(gfc_batch *bt, size_t test, size_t reg, const int32_t *in)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(in);
+		check_test(*bt, test); check_reg(*bt, reg);
+		check_digits(*bt, test, in);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaMemcpyAsync(reg_ptr(*bt, test, reg), in, bt->N * sizeof(int32_t), cudaMemcpyHostToDevice, bt->stream));
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+	});
+}
+
+GFC_API int gfc_batch_get_all(gfc_batch *bt, size_t reg, int32_t *out)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(out);
+		check_reg(*bt, reg);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		// registers of one test are contiguous: reg r of test i at (i * num_regs + r) * N
+		GFC_CK(cudaMemcpy2DAsync(out, bt->N * sizeof(int32_t), reg_ptr(*bt, 0, reg), bt->num_regs * bt->N * sizeof(int32_t),
+								 bt->N * sizeof(int32_t), bt->count, cudaMemcpyDeviceToHost, bt->stream));
+		op_sync(*bt);
+	});
+}
+
+GFC_API int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(in);
+		check_reg(*bt, reg);
+		for (size_t i = 0; i < bt->count; ++i) check_digits(*bt, i, in + i * bt->N);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaMemcpy2DAsync(reg_ptr(*bt, 0, reg), bt->num_regs * bt->N * sizeof(int32_t), in, bt->N * sizeof(int32_t),
+								 bt->N * sizeof(int32_t), bt->count, cudaMemcpyHostToDevice, bt->stream));
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+	});
+}
+
+GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt);
+		if (!plan_valid(bt->n, lr)) fail(GFC_ERR_ARG, "set_plan: invalid plan for this n");
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+		bt->lr = lr;
+		prepare_plan(*bt);
+	});
+}
+
+GFC_API int gfc_batch_plan(const gfc_batch *bt) { return (bt == nullptr) ? GFC_ERR_ARG : bt->lr; }
+
+GFC_API int gfc_batch_widths(const gfc_batch *bt, int32_t *w)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(w);
+		for (size_t i = 0; i < bt->count; ++i) w[i] = (bt->set[i] == 0) ? 2 : 3;
+	});
+}
+
+GFC_API int gfc_batch_sync(gfc_batch *bt)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_sync(*bt); });
+}
+
+GFC_API void *gfc_batch_stream(gfc_batch *bt) { return (bt == nullptr) ? nullptr : static_cast<void *>(bt->stream); }
+
+GFC_API int gfc_batch_capture_begin(gfc_batch *bt)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		GFC_CK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
+		bt->capturing = true;
+	});
+}
+
+GFC_API int gfc_batch_capture_end(gfc_batch *bt, gfc_graph **out)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(out);
+		*out = nullptr;
+		if (!bt->capturing) fail(GFC_ERR_STATE, "capture_end without capture_begin");
+		cudaSetDevice(bt->device);
+		bt->capturing = false;
+		std::unique_ptr<gfc_graph> g(new gfc_graph());
+		g->device = bt->device; g->stream = bt->stream;
+		GFC_CK(cudaStreamEndCapture(bt->stream, &g->graph));
+		GFC_CK(cudaGraphInstantiate(&g->exec, g->graph, 0));
+		*out = g.release();
+	});
+}
+
+GFC_API int gfc_graph_launch(gfc_graph *g)
+{
+	return guard([&] {
+		GFC_NULLCHK(g);
+		cudaSetDevice(g->device);
+		GFC_CK(cudaGraphLaunch(g->exec, g->stream));
+	});
+}
+
+GFC_API void gfc_graph_destroy(gfc_graph *g) { delete g; }

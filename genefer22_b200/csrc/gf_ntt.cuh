@@ -1,0 +1,129 @@
+// gf_ntt.cuh -- negacyclic number-theoretic transform building blocks.
+//
+// The transform of length N = 2^n evaluates a digit polynomial at the N
+// roots of X^N + 1 (the same quotient ring genefer squares in,
+// src/transformCPUi32.h:691-715 and ocl/kernel.cl).  Forward: Cooley-Tukey
+// butterflies (a, b) -> (a + w b, a - w b); inverse: Gentleman-Sande
+// (a, b) -> (a + b, (a - b) / w).  At global stage s (0 <= s < n) element j
+// pairs with j + N/2^(s+1) and uses the root table entry
+//     idx = 2^s + (j >> (n - s)),   W[idx] = psi^bitrev_n(idx)
+// where psi is a primitive 2N-th root of unity.  A sub-transform that covers
+// the stages [s0, s0 + l) of one contiguous block of the global index space
+// is described by its `base` (the block number at stage s0): a column pass of
+// the four-step decomposition has base 1, row k of a row pass has base R + k.
+//
+// Inside a pass, r consecutive stages are done in registers on groups of 2^r
+// elements (radix 2^r); groups are staged through shared memory between
+// passes.
+#pragma once
+
+#include "gf_arith.cuh"
+
+namespace gfc {
+
+template <class Z>
+__device__ __forceinline__ void bfly_ct(uint32_t &a, uint32_t &b, uint32_t w)
+{
+	const uint32_t t = Z::mul(b, w);
+	b = Z::sub(a, t);
+	a = Z::add(a, t);
+}
+
+template <class Z>
+__device__ __forceinline__ void bfly_gs(uint32_t &a, uint32_t &b, uint32_t wi)
+{
+	const uint32_t t = Z::sub(a, b);
+	a = Z::add(a, b);
+	b = Z::mul(t, wi);
+}
+
+// r forward stages on 2^r registers.  Stage t of the group uses the table
+// entries (tbase << t) + sb, sb < 2^t, with tbase = (base << sigma) + blk.
+template <class Z, int r>
+__device__ __forceinline__ void fwd_reg(uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ tw)
+{
+#pragma unroll
+	for (int t = 0; t < r; ++t)
+	{
+		const int half = 1 << (r - 1 - t);
+#pragma unroll
+		for (int sb = 0; sb < (1 << t); ++sb)
+		{
+			const uint32_t w = __ldg(&tw[(tbase << t) + sb]);
+#pragma unroll
+			for (int m = 0; m < half; ++m) bfly_ct<Z>(x[sb * 2 * half + m], x[sb * 2 * half + m + half], w);
+		}
+	}
+}
+
+// r inverse stages (reverse order).  When `norm` is set the group contains
+// global stage 0 (tbase == 1): its butterflies also multiply both outputs by
+// the normalisation, a' = (a + b) c, b' = (a - b) K, with c = twi_fwd0 and
+// K = twi[0] prepared on the host.
+template <class Z, int r>
+__device__ __forceinline__ void inv_reg(uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ twi,
+										bool norm, uint32_t c_norm, uint32_t k_norm)
+{
+#pragma unroll
+	for (int t = r - 1; t >= 0; --t)
+	{
+		const int half = 1 << (r - 1 - t);
+#pragma unroll
+		for (int sb = 0; sb < (1 << t); ++sb)
+		{
+			if ((t == 0) && norm)
+			{
+#pragma unroll
+				for (int m = 0; m < half; ++m)
+				{
+					uint32_t &a = x[m], &b = x[m + half];
+					const uint32_t d = Z::sub(a, b);
+					a = Z::mul(Z::add(a, b), c_norm);
+					b = Z::mul(d, k_norm);
+				}
+			}
+			else
+			{
+				const uint32_t wi = __ldg(&twi[(tbase << t) + sb]);
+#pragma unroll
+				for (int m = 0; m < half; ++m) bfly_gs<Z>(x[sb * 2 * half + m], x[sb * 2 * half + m + half], wi);
+			}
+		}
+	}
+}
+
+// Shared-memory address maps.
+// Rows: `lanes` contiguous transforms of length 2^l, padded one word per 32.
+struct RowMap
+{
+	int l;
+	__device__ __forceinline__ int operator()(int i, int lane) const
+	{
+		const int a = (lane << l) + i;
+		return a + (a >> 5);
+	}
+};
+// Columns: tile [2^l][RS] with the transform index i on the slow axis.
+struct ColMap
+{
+	int RS;
+	__device__ __forceinline__ int operator()(int i, int lane) const { return i * RS + lane; }
+};
+
+// Group geometry of a radix-2^r pass at local stage sigma of a length-2^l
+// transform: group g covers the elements
+//   i_m = (blk << (l - sigma)) + o + (m << (l - sigma - r)),  m < 2^r,
+// with blk = g >> (l - sigma - r), o = g mod 2^(l - sigma - r).
+struct Group
+{
+	int i0, step, blk;
+	__device__ __forceinline__ Group(int g, int l, int sigma, int r)
+	{
+		const int sh = l - sigma - r;
+		blk = g >> sh;
+		i0 = (blk << (l - sigma)) + (g & ((1 << sh) - 1));
+		step = 1 << sh;
+	}
+};
+
+}  // namespace gfc

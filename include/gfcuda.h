@@ -1,0 +1,198 @@
+/*
+ * gfcuda.h -- C ABI of the B200 modular-squaring engine (libgfcuda.so).
+ *
+ * The engine squares numbers modulo b^(2^n) + 1 on an NVIDIA B200
+ * (sm_100a).  It is the drop-in backend for genefer's `transform` interface
+ * (reference: src/transform.h:42-256): each single-test entry point below
+ * replaces one member of that interface, cited beside it.  A genefer-side
+ * `transformCUDA` class (include/transformCUDA.h) forwards to these calls.
+ *
+ * Conventions
+ *   - Every function returns GFC_OK (0) or a negative GFC_ERR_* code and never
+ *     throws; gfc_last_error() gives a message for the calling thread.
+ *   - Registers hold N = 2^n signed digits in natural order (digit i has
+ *     weight b^i), like the int32 vector of genefer's `gint`
+ *     (src/gint.h:17-38).  Digits at rest satisfy |d| <= b/2 + 1; they are
+ *     congruent, not equal, to the reference transform's digits, and
+ *     gint::unbalance maps both to the same canonical residue.
+ *   - Work is enqueued on the handle's CUDA stream (the one passed at
+ *     creation, or a private one).  Calls that move digits to host memory
+ *     synchronise that stream; the others return after enqueueing.
+ *   - A gfc_transform is a batch of one test; the gfc_batch_* calls run many
+ *     tests of the same n in each launch (a throughput extension with no
+ *     counterpart in the reference interface).
+ */
+#ifndef GFCUDA_H
+#define GFCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFC_OK 0
+#define GFC_ERR_ARG (-1)      /* invalid argument (size, register index, b, n) */
+#define GFC_ERR_CUDA (-2)     /* CUDA runtime failure (device, memory, launch) */
+#define GFC_ERR_RANGE (-3)    /* (b, n) outside the exact range of the prime sets */
+#define GFC_ERR_NUMERIC (-4)  /* a device-side carry could not be absorbed */
+#define GFC_ERR_STATE (-5)    /* call not valid in the current state */
+
+typedef struct gfc_batch gfc_batch;
+typedef struct gfc_batch gfc_transform;
+typedef struct gfc_graph gfc_graph;
+
+/* Message of the last failing call on this thread. */
+const char *gfc_last_error(void);
+
+/* Library version as major*10000 + minor*100 + patch. */
+int gfc_version(void);
+
+/* ------------------------------------------------------------------ single test
+ * Replaces transform::create_gpu / create_ocl (src/transform.h:114-120,
+ * src/transform_ocl.cpp:20-51) and the transformGPUs constructor
+ * (src/transformGPU.h:945-1083).  b: base, 2 <= b < 2^31; n: 10 <= n <= 23;
+ * num_regs: registers (3 for quick tests, src/genefer.h:1384); device: CUDA
+ * ordinal; stream: cudaStream_t to use, or NULL for a private stream. */
+int gfc_create(uint32_t b, uint32_t n, size_t num_regs, int device, void *stream, gfc_transform **out);
+
+/* Releases all device memory (transformGPUs destructor, src/transformGPU.h:1085-1093). */
+void gfc_destroy(gfc_transform *t);
+
+/* r_0 = a  (transform::set, src/transform.h:58).  Requires a <= b/2. */
+int gfc_set(gfc_transform *t, uint32_t a);
+
+/* r_0 = r_0^2, or 2 r_0^2 when dup != 0  (transform::squareDup, src/transform.h:59). */
+int gfc_square_dup(gfc_transform *t, int dup);
+
+/* r_m = transform(r_src)  (transform::initMultiplicand, src/transform.h:61). */
+int gfc_init_multiplicand(gfc_transform *t, size_t src);
+
+/* r_0 = r_0 * r_m  (transform::mul, src/transform.h:62). */
+int gfc_mul(gfc_transform *t);
+
+/* r_dst = r_src  (transform::copy, src/transform.h:64). */
+int gfc_copy(gfc_transform *t, size_t dst, size_t src);
+
+/* Reads r_0 as N signed digits into host memory; synchronises
+ * (transform::getZi via getInt, src/transform.h:54, :234-239). */
+int gfc_get_zi(gfc_transform *t, int32_t *zi);
+
+/* Writes r_0 from N host digits with |d| <= b/2, e.g. after gint::balance
+ * (transform::setZi via setInt, src/transform.h:55, :241-246). */
+int gfc_set_zi(gfc_transform *t, const int32_t *zi);
+
+/* Device bytes held by the handle (transform::getMemSize, src/transform.h:66). */
+size_t gfc_get_mem_size(const gfc_transform *t);
+
+/* Bytes of state touched per squaring (transform::getCacheSize, src/transform.h:67). */
+size_t gfc_get_cache_size(const gfc_transform *t);
+
+/* Context payload (transform::saveContext / readContext, src/transform.h:69-70,
+ * src/transformGPU.h:1127-1150): a tag word (GFC_CONTEXT_KIND) followed by
+ * num_regs registers of N int32 digits.  gfc_context_size gives the byte size;
+ * gfc_save_context synchronises; gfc_read_context returns GFC_ERR_STATE when
+ * the tag or size does not match (readContext returning false). */
+#define GFC_CONTEXT_KIND 0x47464342 /* "GFCB" */
+size_t gfc_context_size(const gfc_transform *t, size_t num_regs);
+int gfc_save_context(gfc_transform *t, void *buf, size_t size, size_t num_regs);
+int gfc_read_context(gfc_transform *t, const void *buf, size_t size, size_t num_regs);
+
+/* Number of RNS primes (2 or 3) chosen for (b, n); the analogue of the
+ * transform kind NTT2/NTT3 (src/transform.h:45, src/transform_ocl.cpp:35-50). */
+int gfc_width(const gfc_transform *t);
+
+/* Waits for all enqueued work; returns GFC_ERR_NUMERIC if a device-side check
+ * failed since the last call. */
+int gfc_sync(gfc_transform *t);
+
+/* ------------------------------------------------------------------ batches of tests */
+
+/* count tests of the same n with bases b[0..count-1] (each test picks its own
+ * RNS width), num_regs registers each. */
+int gfc_batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_regs, int device, void *stream,
+					 gfc_batch **out);
+void gfc_batch_destroy(gfc_batch *bt);
+size_t gfc_batch_count(const gfc_batch *bt);
+
+/* Per-test r_0 = a, r_dst = r_src, for all tests. */
+int gfc_batch_set(gfc_batch *bt, uint32_t a);
+int gfc_batch_copy(gfc_batch *bt, size_t dst, size_t src);
+
+/* count squarings of r_0 for every test with a fixed dup flag. */
+int gfc_batch_square(gfc_batch *bt, int dup, uint32_t count);
+
+/* Uploads test `test`'s exponent (nbits bits, little-endian 32-bit words)
+ * and sets its bit position to nbits - 1. */
+int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *words, uint64_t nbits);
+
+/* Sets every test's bit position (pos[i] < 0: the test has finished). */
+int gfc_batch_set_pos(gfc_batch *bt, const int64_t *pos);
+int gfc_batch_get_pos(gfc_batch *bt, int64_t *pos);
+
+/* count squarings per test, squaring i using dup = bit (pos - i) of the
+ * test's exponent, then pos -= count; tests whose position goes below zero
+ * stop (the loop body of genefer::prp, src/genefer.h:508-527). */
+int gfc_batch_square_exp(gfc_batch *bt, uint32_t count);
+
+/* r_m = transform(r_src) and r_dst = r_0 * r_m, for all tests. */
+int gfc_batch_init_multiplicand(gfc_batch *bt, size_t src);
+int gfc_batch_mul(gfc_batch *bt, size_t dst);
+
+/* Gerbicz-Li update d(t) <- d(t) * r for all tests: r_1 = r_0 * r_1 with r_0
+ * unchanged; the same result as copy(2,0); mul(1); copy(1,0); copy(0,2)
+ * (src/genefer.h:529-535) without the copies. */
+int gfc_batch_gl_step(gfc_batch *bt);
+
+/* Digits of register `reg` of one test, or of all tests (count x N). */
+int gfc_batch_get_zi(gfc_batch *bt, size_t test, size_t reg, int32_t *out);
+int gfc_batch_set_zi(gfc_batch *bt, size_t test, size_t reg, const int32_t *in);
+int gfc_batch_get_all(gfc_batch *bt, size_t reg, int32_t *out);
+int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
+
+/* Kernel plan.  lr = 0: one CTA per test with the state in shared memory
+ * (n <= 14); lr > 0: four-step with R = 2^lr rows (3 <= lr <= 10,
+ * 8 <= n - lr <= 13).  gfc_batch_plan reads the current plan. */
+int gfc_batch_set_plan(gfc_batch *bt, int lr);
+int gfc_batch_plan(const gfc_batch *bt);
+
+/* Per-test RNS width (2 or 3), into w[0..count-1]. */
+int gfc_batch_widths(const gfc_batch *bt, int32_t *w);
+
+/* Waits for all enqueued work (see gfc_sync). */
+int gfc_batch_sync(gfc_batch *bt);
+
+/* CUDA stream of the batch (cudaStream_t). */
+void *gfc_batch_stream(gfc_batch *bt);
+
+/* CUDA graphs: calls between capture_begin and capture_end are recorded (not
+ * run) and replayed by gfc_graph_launch on the batch's stream. */
+int gfc_batch_capture_begin(gfc_batch *bt);
+int gfc_batch_capture_end(gfc_batch *bt, gfc_graph **out);
+int gfc_graph_launch(gfc_graph *g);
+void gfc_graph_destroy(gfc_graph *g);
+
+/* Kernel launches issued by this process so far (all handles). */
+uint64_t gfc_launch_count(void);
+
+/* ------------------------------------------------------------------ residues (host)
+ * genefer's gint utilities on N host digits (src/gint.h:40-225). */
+
+/* gint::unbalance: canonical digits in [0, b) (src/gint.h:40-102). */
+void gfc_gint_unbalance(int32_t *d, size_t size, uint32_t b);
+
+/* gint::balance: digits in (-b/2, b/2] (src/gint.h:104-149). */
+void gfc_gint_balance(int32_t *d, size_t size, uint32_t b);
+
+/* gint::isOne on canonical digits; writes res64 and old64 (src/gint.h:169-202). */
+int gfc_gint_is_one(const int32_t *d, size_t size, uint32_t b, uint64_t *res64, uint64_t *old64);
+
+/* gint::gethash64 on canonical digits (src/gint.h:204-219). */
+uint64_t gfc_gint_hash64(const int32_t *d, size_t size);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GFCUDA_H */
