@@ -1,0 +1,360 @@
+"""Benchmark of the modular-squaring engine (one JSON line on rank 0).
+
+Workload (default): a batch of 64 Fermat PRP tests of b^(2^16) + 1, b even,
+seeded uniform in [10^6, 10^8] (seed 1002), run as Gerbicz-Li blocks of 1000
+squarings; one step = one block (1000 squarings of every test + the d(t)
+update), replayed from a CUDA graph.  Metric: digit-squarings per second
+(sum over tests of 2^n x squarings / time; the Gerbicz-Li products are timed
+but not counted).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU transforms (oracle/_ref, the
+reference sources compiled here) on the host cores for the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_LOG = 16
+COUNT = 64
+BLOCK = 1000
+SEED = 1002
+B_LO, B_HI = 10**6, 10**8
+METRIC = "digit-squarings/s"
+WORKLOAD = "batch of 64 Fermat PRP tests b^(2^16)+1, b even uniform [1e6,1e8] seed 1002, Gerbicz-Li block of 1000 squarings"
+
+
+def bases(seed: int = SEED, count: int = COUNT):
+    rng = np.random.default_rng(seed)
+    return (rng.integers(B_LO // 2, B_HI // 2 + 1, size=count) * 2).astype(np.int64).tolist()
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_info():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ------------------------------------------------------------------ reference CPU path
+
+def cpu_reference(n: int, test_bases, seconds: float, impl: str = ""):
+    """The reference's CPU transform (transform::create_cpu, src/transform.h:122-193,
+    built from the reference sources into oracle/_ref) on the host cores.  One test
+    per worker thread, several threads per test when there are more cores than
+    tests; every worker runs squareDup on its own test for ~`seconds`.
+    Returns (digit-squarings/s, cores, sample description, transform type)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gf_oracle as G
+    if not G.ref_available():
+        raise RuntimeError("oracle/_ref/libgfref.so not built")
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    workers = max(1, min(cores, len(test_bases)))
+    tpt = 1 if impl == "i32" else max(1, cores // workers)
+    rng = np.random.default_rng(7)
+    trs = []
+    for i in range(workers):
+        b = int(test_bases[i])
+        t = G.RefTransform(b, n, num_regs=3, impl=impl, threads=tpt)
+        t.setInt(rng.integers(-(b // 2), b // 2 + 1, size=1 << n).astype(np.int32))
+        trs.append(t)
+    # calibrate the per-worker squaring count on one worker alone
+    t0 = time.perf_counter()
+    trs[0].run_squarings(np.ones(4, np.uint8))
+    per = max((time.perf_counter() - t0) / 4, 1e-6)
+    sq = max(4, int(seconds / per))
+    bits = (np.arange(sq) % 2).astype(np.uint8)
+    th = [threading.Thread(target=t.run_squarings, args=(bits,)) for t in trs]
+    t0 = time.perf_counter()
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    dt = time.perf_counter() - t0
+    value = workers * (1 << n) * sq / dt
+    sample = f"{workers} tests x {sq} squarings at n={n} ({tpt} thread(s) each), {dt:.1f} s"
+    return value, workers * tpt, sample, trs[0].ttype
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    bs = bases()
+    per_step = 3.0
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, cores, sample, ttype = cpu_reference(N_LOG, bs, per_step)
+        if k >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    ms = COUNT * (1 << N_LOG) * BLOCK / value * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if ttype != "i32" else "u32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "n": N_LOG, "tests": COUNT, "block": BLOCK,
+                                            "seed": SEED, "reference_transform": ttype},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def algorithmic(kind: int, widths: np.ndarray, n: int, lr: int):
+    """Algorithmic DRAM bytes and radix-2 butterflies of one launch of kernel
+    kind `kind` (see Batch.time_kernels) over all tests of the batch."""
+    N = 1 << n
+    W = widths.astype(np.float64)
+    lc = n - lr
+    if kind == 1:   # column forward: read digits, write W planes; lr stages
+        return float(np.sum(4 * N + 4 * W * N)), float(np.sum(W * (N / 2) * lr))
+    if kind == 2:   # rows: read + write W planes; 2 lc stages + pointwise
+        return float(np.sum(8 * W * N)), float(np.sum(W * (N / 2) * 2 * lc + W * N))
+    if kind == 3:   # column inverse + CRT + carry: read W planes, write digits and carries
+        return float(np.sum(4 * W * N + 4 * N + 8 * N / 16)), float(np.sum(W * (N / 2) * lr))
+    if kind == 4:   # carry fix-up: read carries
+        return float(np.sum(8 * N / 16 + 0 * W)), 0.0
+    # single-CTA squaring: digits in and out; the whole transform in shared memory
+    return float(np.sum(8 * N + 0 * W)), float(np.sum(W * (N / 2) * 2 * n + W * N))
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from genefer22_b200 import Batch, Transform, _lib
+    from genefer22_b200 import genefer as gf
+
+    L = _lib.lib()
+    bs = bases(SEED + rank)
+    bt = Batch(bs, N_LOG, num_regs=3, device=local)
+    widths = bt.widths()
+    runner = gf.BatchPRP(bt, B=BLOCK)
+    runner.load()
+    first = runner.schedule()[0]
+    bt.square_exp(first)          # align to the Gerbicz-Li block boundary
+    bt.gl_step()
+    g = runner.block_graph()
+    stream = torch.cuda.ExternalStream(bt.stream, device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        g.launch()
+    bt.sync()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = L.gfc_launch_count()
+    with Clocks(local) as ck:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()     # L2 flush between timed steps (outside the events)
+            ev[k][0].record(stream)
+            g.launch()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    launches = int(L.gfc_launch_count() - l0)
+    if dist is not None:
+        dist.barrier()
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    digits_per_step = world * COUNT * (1 << N_LOG) * BLOCK
+    value = digits_per_step * args.steps / (total_ms * 1e-3)
+
+    # end to end through the public API: host digits in (pinned), one block, host digits out
+    pin0 = torch.empty((COUNT, 1 << N_LOG), dtype=torch.int32, pin_memory=True).numpy()
+    pin1 = torch.empty((COUNT, 1 << N_LOG), dtype=torch.int32, pin_memory=True).numpy()
+    bt.get_all(0, out=pin0)
+    bt.get_all(1, out=pin1)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        bt.put_all(pin0, 0)
+        bt.put_all(pin1, 1)
+        g.launch()
+        bt.get_all(0, out=pin0)
+        bt.get_all(1, out=pin1)
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = digits_per_step * args.steps / e2e_s
+    io_bytes = 2 * COUNT * (1 << N_LOG) * 4
+
+    if rank != 0:
+        if dist is not None:
+            del g
+            dist.destroy_process_group()
+        return
+
+    # per-kernel durations (CUDA events on the batch's stream) -> roofline of the dominant kernel
+    lr = bt.plan()
+    kms = bt.time_kernels(5)
+    dom = int(np.argmax(kms))
+    names = ["k_small", "k_col_fwd", "k_row", "k_col_inv", "k_fixup"]
+    abytes, abfly = algorithmic(dom, widths, N_LOG, lr)
+    hbm, hbm_kind = peaks()
+    achieved = abytes / (kms[dom] * 1e-3) / 1e9
+    probe = (ctypes.c_double * 4)()
+    L.gfc_probe_int_throughput(local, probe)
+    frac_w3 = float(np.mean(widths == 3))
+    bfly_peak = frac_w3 * probe[3] + (1 - frac_w3) * probe[2]
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tj):
+        with open(tj) as f:
+            traffic = json.load(f).get(f"{names[dom]}_lr{lr}_n{N_LOG}_x{COUNT}")
+
+    # plain path: one test, one squareDup call per squaring from the host
+    tr = Transform(int(bs[0]), N_LOG)
+    tr.set(3)
+    for _ in range(20):
+        tr.squareDup(False)
+    tr.sync()
+    kp = 300
+    t0 = time.perf_counter()
+    for i in range(kp):
+        tr.squareDup(i % 2 == 1)
+    tr.sync()
+    plain = (1 << N_LOG) * kp / (time.perf_counter() - t0)
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        try:
+            v, cores, sample, ttype = cpu_reference(N_LOG, bs, args.cpu_seconds)
+            cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "reference",
+                   "sample": f"reference {ttype} transform: {sample}"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": METRIC, "cores": None, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": N_LOG, "tests_per_gpu": COUNT, "block": BLOCK, "seed": SEED,
+                   "plan_lr": lr, "rns_widths": {"2": int(np.sum(widths == 2)), "3": int(np.sum(widths == 3))},
+                   "l2": "256 MB buffer written between timed steps", "graph": "one CUDA graph per block"},
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": abytes, "launch_ms": float(kms[dom]),
+                     "int_pipe": {"achieved_bfly_per_s": abfly / (kms[dom] * 1e-3), "peak_bfly_per_s": bfly_peak,
+                                  "frac": abfly / (kms[dom] * 1e-3) / bfly_peak,
+                                  "peak_kind": "measured (gfc_probe_int_throughput)"},
+                     "kernel_ms": {nm: float(x) for nm, x in zip(names, kms)}},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+        "gpu_launches": launches,
+        "clocks": ck.summary(),
+        "plain": {"value": plain, "unit": METRIC, "what": "one test, one gfc_square_dup call per squaring"},
+        "batched_over_plain": value / world / plain,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        del g
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -63,12 +63,14 @@ SIGNATURES = {
     "gfc_batch_plan": (ctypes.c_int, [vp]),
     "gfc_batch_widths": (ctypes.c_int, [vp, c_i32p]),
     "gfc_batch_sync": (ctypes.c_int, [vp]),
+    "gfc_batch_time_kernels": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float)]),
     "gfc_batch_stream": (vp, [vp]),
     "gfc_batch_capture_begin": (ctypes.c_int, [vp]),
     "gfc_batch_capture_end": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
     "gfc_graph_launch": (ctypes.c_int, [vp]),
     "gfc_graph_destroy": (None, [vp]),
     "gfc_launch_count": (ctypes.c_uint64, []),
+    "gfc_probe_int_throughput": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gfc_gint_unbalance": (None, [c_i32p, ctypes.c_size_t, ctypes.c_uint32]),
     "gfc_gint_balance": (None, [c_i32p, ctypes.c_size_t, ctypes.c_uint32]),
     "gfc_gint_is_one": (ctypes.c_int, [c_i32p, ctypes.c_size_t, ctypes.c_uint32, c_u64p, c_u64p]),

@@ -14,7 +14,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libgfcuda.so")
-SOURCES = [os.path.join(CSRC, "gf_host.cu"), os.path.join(CSRC, "gf_gint.cpp")]
+SOURCES = [os.path.join(CSRC, "gf_host.cu"), os.path.join(CSRC, "gf_probe.cu"), os.path.join(CSRC, "gf_gint.cpp")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("gf_arith.cuh", "gf_ntt.cuh", "gf_kernels.cuh")] + \
     [os.path.join(ROOT, "include", "gfcuda.h")]
 

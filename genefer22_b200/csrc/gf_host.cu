@@ -316,6 +316,7 @@ struct gfc_batch
 	std::vector<uint32_t *> ebits;
 	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };
 	bool capturing = false;
+	uint64_t capture_start = 0;   // launch counter at capture_begin
 
 	~gfc_batch()
 	{
@@ -332,6 +333,7 @@ struct gfc_graph
 	cudaStream_t stream = nullptr;
 	cudaGraph_t graph = nullptr;
 	cudaGraphExec_t exec = nullptr;
+	uint64_t kernels = 0;         // kernel nodes recorded
 	~gfc_graph()
 	{
 		cudaSetDevice(device);
@@ -388,6 +390,14 @@ void prepare_plan(gfc_batch &bt)
 	}
 }
 
+void launch_fixup(gfc_batch &bt, const Args &a, int g)
+{
+	const unsigned nseg = static_cast<unsigned>(bt.N / SEG);
+	const dim3 grid((nseg + FIX_THREADS - 1) / FIX_THREADS, static_cast<unsigned>(g));
+	k_fixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
+	after_launch();
+}
+
 // Four-step squaring / product / forward transform for the tests of one set.
 void fourstep(gfc_batch &bt, int s, const Args &a)
 {
@@ -396,10 +406,7 @@ void fourstep(gfc_batch &bt, int s, const Args &a)
 	launch_row(s, bt.n - bt.lr, a, g, bt.stream, false);
 	if (a.op == OP_FWD) return;
 	launch_col(s, bt.lr, true, a, g, bt.stream, false);
-	const unsigned nseg = static_cast<unsigned>(bt.N / SEG);
-	const dim3 grid((nseg + FIX_THREADS - 1) / FIX_THREADS, static_cast<unsigned>(g));
-	k_fixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
-	after_launch();
+	launch_fixup(bt, a, g);
 }
 
 // count squarings of r_0 (dup_mode DUP_NONE / DUP_ALL / DUP_BITS).
@@ -459,6 +466,55 @@ void op_mul(gfc_batch &bt, size_t dst)
 		if (bt.lr == 0) launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
 		else fourstep(bt, s, a);
 	}
+}
+
+// One squaring at a time with events around each kernel (see gfc_batch_time_kernels).
+void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
+{
+	no_capture(bt);
+	cudaEvent_t ev[5];
+	for (auto &e : ev) GFC_CK(cudaEventCreate(&e));
+	double acc[5] = { 0, 0, 0, 0, 0 };
+	auto span = [&](int i, int j) { float t = 0; GFC_CK(cudaEventElapsedTime(&t, ev[i], ev[j])); return static_cast<double>(t); };
+	try
+	{
+		for (uint32_t r = 0; r < reps; ++r)
+			for (int s = 0; s < 2; ++s)
+			{
+				if (bt.nset[s] == 0) continue;
+				Args a = make_args(bt, s);
+				a.op = OP_SQUARE; a.dup_mode = DUP_NONE; a.count = 1; a.src = 0; a.dst = 0;
+				const int g = bt.nset[s];
+				GFC_CK(cudaEventRecord(ev[0], bt.stream));
+				if (bt.lr == 0)
+				{
+					launch_small(s, bt.n, a, g, bt.stream, false);
+					GFC_CK(cudaEventRecord(ev[1], bt.stream));
+					GFC_CK(cudaEventSynchronize(ev[1]));
+					acc[0] += span(0, 1);
+				}
+				else
+				{
+					launch_col(s, bt.lr, false, a, g, bt.stream, false);
+					GFC_CK(cudaEventRecord(ev[1], bt.stream));
+					launch_row(s, bt.n - bt.lr, a, g, bt.stream, false);
+					GFC_CK(cudaEventRecord(ev[2], bt.stream));
+					launch_col(s, bt.lr, true, a, g, bt.stream, false);
+					GFC_CK(cudaEventRecord(ev[3], bt.stream));
+					launch_fixup(bt, a, g);
+					GFC_CK(cudaEventRecord(ev[4], bt.stream));
+					GFC_CK(cudaEventSynchronize(ev[4]));
+					acc[1] += span(0, 1); acc[2] += span(1, 2); acc[3] += span(2, 3); acc[4] += span(3, 4);
+				}
+			}
+	}
+	catch (...)
+	{
+		for (auto &e : ev) cudaEventDestroy(e);
+		throw;
+	}
+	for (auto &e : ev) cudaEventDestroy(e);
+	for (int i = 0; i < 5; ++i) ms[i] = static_cast<float>(acc[i] / (reps ? reps : 1));
 }
 
 Args all_args(const gfc_batch &bt)
@@ -899,6 +955,11 @@ GFC_API int gfc_batch_widths(const gfc_batch *bt, int32_t *w)
 	});
 }
 
+GFC_API int gfc_batch_time_kernels(gfc_batch *bt, uint32_t reps, float *ms)
+{
+	return guard([&] { GFC_NULLCHK(bt); GFC_NULLCHK(ms); cudaSetDevice(bt->device); time_kernels(*bt, reps, ms); });
+}
+
 GFC_API int gfc_batch_sync(gfc_batch *bt)
 {
 	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_sync(*bt); });
@@ -914,6 +975,7 @@ GFC_API int gfc_batch_capture_begin(gfc_batch *bt)
 		cudaSetDevice(bt->device);
 		GFC_CK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
 		bt->capturing = true;
+		bt->capture_start = g_launches.load();
 	});
 }
 
@@ -927,6 +989,9 @@ GFC_API int gfc_batch_capture_end(gfc_batch *bt, gfc_graph **out)
 		bt->capturing = false;
 		std::unique_ptr<gfc_graph> g(new gfc_graph());
 		g->device = bt->device; g->stream = bt->stream;
+		// recorded launches are counted when the graph runs, not here
+		g->kernels = g_launches.load() - bt->capture_start;
+		g_launches.fetch_sub(g->kernels);
 		GFC_CK(cudaStreamEndCapture(bt->stream, &g->graph));
 		GFC_CK(cudaGraphInstantiate(&g->exec, g->graph, 0));
 		*out = g.release();
@@ -939,6 +1004,7 @@ GFC_API int gfc_graph_launch(gfc_graph *g)
 		GFC_NULLCHK(g);
 		cudaSetDevice(g->device);
 		GFC_CK(cudaGraphLaunch(g->exec, g->stream));
+		g_launches.fetch_add(g->kernels);
 	});
 }
 

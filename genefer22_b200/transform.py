@@ -36,8 +36,11 @@ class Batch:
     def close(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().gfc_batch_destroy(h)
             self._h = None
+            try:
+                lib().gfc_batch_destroy(h)
+            except Exception:   # interpreter shutdown
+                pass
 
     __del__ = close
 
@@ -122,6 +125,13 @@ class Batch:
     def sync(self):
         check(lib().gfc_batch_sync(self._h))
 
+    def time_kernels(self, reps: int = 5) -> np.ndarray:
+        """Mean ms per squaring of each kernel kind: [single-CTA, column-forward,
+        row, column-inverse + carry, carry fix-up]."""
+        ms = (ctypes.c_float * 5)()
+        check(lib().gfc_batch_time_kernels(self._h, reps, ms))
+        return np.array(list(ms), dtype=np.float64)
+
     def capture(self, fn) -> "Graph":
         """Records the batch calls made by fn() into a CUDA graph."""
         check(lib().gfc_batch_capture_begin(self._h))
@@ -144,8 +154,11 @@ class Graph:
     def close(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().gfc_graph_destroy(h)
             self._h = None
+            try:
+                lib().gfc_graph_destroy(h)
+            except Exception:   # interpreter shutdown
+                pass
 
     __del__ = close
 

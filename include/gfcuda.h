@@ -173,8 +173,22 @@ int gfc_batch_capture_end(gfc_batch *bt, gfc_graph **out);
 int gfc_graph_launch(gfc_graph *g);
 void gfc_graph_destroy(gfc_graph *g);
 
-/* Kernel launches issued by this process so far (all handles). */
+/* Kernel launches issued by this process so far (all handles; a graph replay
+ * counts the kernels it contains). */
 uint64_t gfc_launch_count(void);
+
+/* Kernel timing (no counterpart in the reference): runs `reps` squarings of
+ * all tests (dup = 0) with a CUDA event recorded on the batch's stream around
+ * every kernel, and returns the mean duration of each kernel kind in ms:
+ * ms[0] single-CTA kernel (plan 0), ms[1] column-forward, ms[2] row,
+ * ms[3] column-inverse + carry, ms[4] carry fix-up (0 when unused). */
+int gfc_batch_time_kernels(gfc_batch *bt, uint32_t reps, float *ms);
+
+/* Integer-pipe probe (no counterpart in the reference): Montgomery products
+ * and radix-2 butterflies per second on `device`, out[0..3] = product with
+ * the 32-bit primes, product with the 31-bit primes, butterfly 32-bit,
+ * butterfly 31-bit.  The roofline denominator for the squaring kernels. */
+int gfc_probe_int_throughput(int device, double *out);
 
 /* ------------------------------------------------------------------ residues (host)
  * genefer's gint utilities on N host digits (src/gint.h:40-225). */
