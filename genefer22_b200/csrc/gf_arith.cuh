@@ -102,6 +102,54 @@ struct Zp
 	}
 };
 
+// The same arithmetic with the prime held in registers, so that one code path
+// serves every plane of a prime set (smaller kernels, fewer i-cache misses).
+template <bool P31>
+struct ZpR
+{
+	uint32_t p, q;
+
+	__device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b) const
+	{
+		const uint32_t s = a + b;
+		if (P31) return min(s, s - p);
+		return (a >= p - b) ? s - p : s;
+	}
+
+	__device__ __forceinline__ uint32_t sub(uint32_t a, uint32_t b) const
+	{
+		const uint32_t d = a - b;
+		if (P31) return min(d, d + p);
+		return (a < b) ? d + p : d;
+	}
+
+	__device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const
+	{
+		const uint64_t t = static_cast<uint64_t>(a) * b;
+		const uint32_t lo = static_cast<uint32_t>(t), hi = static_cast<uint32_t>(t >> 32);
+		const uint32_t mh = __umulhi(lo * q, p);
+		const uint32_t u = hi - mh;
+		if (P31) return min(u, u + p);
+		return (hi < mh) ? u + p : u;
+	}
+
+	__device__ __forceinline__ uint32_t from_int(int32_t d) const
+	{
+		return static_cast<uint32_t>(d) + ((d < 0) ? p : 0u);
+	}
+};
+
+// Plane `pl` of prime set SET as register-held arithmetic.
+template <int SET>
+__device__ __forceinline__ ZpR<PrimeSet<SET>::P31> prime_rt(int pl)
+{
+	constexpr uint32_t p0 = PrimeSet<SET>::p[0], p1 = PrimeSet<SET>::p[1], p2 = PrimeSet<SET>::p[2];
+	ZpR<PrimeSet<SET>::P31> z;
+	z.p = (pl == 0) ? p0 : ((pl == 1) ? p1 : p2);
+	z.q = (pl == 0) ? mont_qinv(p0) : ((pl == 1) ? mont_qinv(p1) : mont_qinv(p2));
+	return z;
+}
+
 // ---------------------------------------------------------------- CRT (Garner)
 
 // Host-side constants, computed once per prime set.
@@ -125,42 +173,7 @@ struct Crt<1>
 	static constexpr uint32_t c123 = to_mont_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);   // (p1 p2)^{-1} mod p3
 };
 
-// The centred integer v with |v| < M/2 from its residues (normal form).
-template <int SET>
-__device__ __forceinline__ i128 crt(const uint32_t x[3]);
-
-template <>
-__device__ __forceinline__ i128 crt<0>(const uint32_t x[3])
-{
-	using C = Crt<0>;
-	using Z2 = Zp<C::p2, false>;
-	const uint32_t x1m2 = (x[0] >= C::p2) ? x[0] - C::p2 : x[0];
-	const uint32_t a2 = Z2::mul(Z2::sub(x[1], x1m2), C::c12);
-	const uint64_t v = static_cast<uint64_t>(a2) * C::p1 + x[0];
-	constexpr uint64_t M = static_cast<uint64_t>(C::p1) * C::p2;
-	return (v > M / 2) ? static_cast<i128>(v) - static_cast<i128>(M) : static_cast<i128>(v);
-}
-
-template <>
-__device__ __forceinline__ i128 crt<1>(const uint32_t x[3])
-{
-	using C = Crt<1>;
-	using Z2 = Zp<C::p2, true>;
-	using Z3 = Zp<C::p3, true>;
-	const uint32_t x1m2 = (x[0] >= C::p2) ? x[0] - C::p2 : x[0];
-	const uint32_t a2 = Z2::mul(Z2::sub(x[1], x1m2), C::c12);
-	// a3 = (x3 - x1 - a2 p1) / (p1 p2) mod p3
-	const uint32_t x1m3 = (x[0] >= C::p3) ? x[0] - C::p3 : x[0];
-	const uint32_t t = Z3::add(x1m3, Z3::mul(a2, C::p1m3));
-	const uint32_t a3 = Z3::mul(Z3::sub(x[2], t), C::c123);
-	// v = x1 + p1 (a2 + p2 a3)
-	const uint64_t h = static_cast<uint64_t>(a3) * C::p2 + a2;
-	const u128 v = static_cast<u128>(h) * C::p1 + x[0];
-	constexpr u128 M = static_cast<u128>(static_cast<uint64_t>(C::p1) * C::p2) * C::p3;
-	return (v > M / 2) ? static_cast<i128>(v) - static_cast<i128>(M) : static_cast<i128>(v);
-}
-
-// ---------------------------------------------------------------- base-b digit extraction
+// ---------------------------------------------------------------- CRT + base-b carry
 
 // Division by a fixed base b (2 <= b < 2^31) with the 64-bit reciprocal
 // binv = floor((2^64 - 1) / b): for n < 2^64, q = mulhi(n, binv) is floor(n/b)
@@ -174,29 +187,73 @@ __device__ __forceinline__ uint64_t divb64(uint64_t n, uint32_t b, uint64_t binv
 	return q;
 }
 
-// Balanced digit of s in [-b/2, b/2) and carry floor((s + b/2) / b),
-// for |s| < 2^95 (b even; for odd b the digit lies in [-(b-1)/2, (b+1)/2)).
-__device__ __forceinline__ int32_t digit_carry(i128 s, uint32_t b, uint64_t binv, int64_t &carry)
+// Per-test constants of the fused CRT + carry, computed on the host.
+// With f = 1 (square) or 2 (dup), T the top mixed-radix weight of the prime
+// set (p1 for set 0, p1 p2 for set 1) and M the product of its primes:
+//   q[f-1] = floor(f T / b), r[f-1] = f T mod b,
+//   mq[f-1] = floor(f M / b) mod 2^64, mr[f-1] = f M mod b,
+//   K = ceil(2^56 / b), kb = K b.
+struct CarryK
 {
-	const uint32_t h = b / 2;
-	const i128 t = s + h;
-	const bool neg = (t < 0);
-	const u128 a = static_cast<u128>(neg ? ~t : t);   // -t-1 when negative
-	const uint64_t lo = static_cast<uint64_t>(a), hi = static_cast<uint64_t>(a >> 64);
-	uint64_t r1, r0;
-	const uint64_t q1 = divb64((hi << 32) | (lo >> 32), b, binv, r1);
-	const uint64_t q0 = divb64((r1 << 32) | (lo & 0xffffffffu), b, binv, r0);
-	uint64_t q = (q1 << 32) + q0;
-	uint32_t r = static_cast<uint32_t>(r0);
-	if (neg) { q = ~q; r = b - 1 - r; }
-	carry = static_cast<int64_t>(q);
-	return static_cast<int32_t>(r) - static_cast<int32_t>(h);
+	uint64_t binv, kb, k;
+	uint64_t q[2], mq[2];
+	uint32_t r[2], mr[2];
+	uint32_t b, h;
+};
+
+// Balanced digit in [-b/2, b/2) of f v + c, where v is the centred CRT value
+// of the residues x (|v| < M/2), and the carry floor((f v + c + b/2) / b)
+// written back to c.  Garner's mixed radix v = x1 + p1 a2 (+ p1 p2 a3) is
+// split as  f v + c + b/2 = U + c + b (Q top - z (mq + 1))  with the top term
+// f T top = (Q b + R) top folded into U < 2^64, so one 64-bit division by b
+// remains; the quotient is assembled modulo 2^64, which is exact because the
+// carry of a resting register is below 2^55 in magnitude.
+template <int SET>
+__device__ __forceinline__ int32_t crt_carry(const uint32_t x[3], int dup, const CarryK &K, int64_t &c);
+
+template <>
+__device__ __forceinline__ int32_t crt_carry<0>(const uint32_t x[3], int dup, const CarryK &K, int64_t &c)
+{
+	using C = Crt<0>;
+	using Z2 = Zp<C::p2, false>;
+	constexpr uint64_t M = static_cast<uint64_t>(C::p1) * C::p2;
+	const uint32_t x1m2 = (x[0] >= C::p2) ? x[0] - C::p2 : x[0];
+	const uint32_t a2 = Z2::mul(Z2::sub(x[1], x1m2), C::c12);
+	const bool z = (static_cast<uint64_t>(a2) * C::p1 + x[0]) > M / 2;
+	const uint64_t U = (static_cast<uint64_t>(x[0]) << dup) + static_cast<uint64_t>(K.r[dup]) * a2 + K.h + (z ? K.b - K.mr[dup] : 0u);
+	uint64_t rv;
+	const uint64_t qv = divb64(U + static_cast<uint64_t>(c) + K.kb, K.b, K.binv, rv);
+	c = static_cast<int64_t>(qv + K.q[dup] * a2 - (z ? K.mq[dup] + 1 : 0) - K.k);
+	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
 }
 
-// Same for a 64-bit signed value (used when absorbing a carry into a digit).
-__device__ __forceinline__ int32_t digit_carry64(int64_t s, uint32_t b, uint64_t binv, int64_t &carry)
+template <>
+__device__ __forceinline__ int32_t crt_carry<1>(const uint32_t x[3], int dup, const CarryK &K, int64_t &c)
 {
-	return digit_carry(static_cast<i128>(s), b, binv, carry);
+	using C = Crt<1>;
+	using Z2 = Zp<C::p2, true>;
+	using Z3 = Zp<C::p3, true>;
+	constexpr uint64_t P12 = static_cast<uint64_t>(C::p1) * C::p2;
+	const uint32_t x1m2 = (x[0] >= C::p2) ? x[0] - C::p2 : x[0];
+	const uint32_t a2 = Z2::mul(Z2::sub(x[1], x1m2), C::c12);
+	const uint32_t x1m3 = (x[0] >= C::p3) ? x[0] - C::p3 : x[0];
+	const uint32_t a3 = Z3::mul(Z3::sub(x[2], Z3::add(x1m3, Z3::mul(a2, C::p1m3))), C::c123);
+	const uint64_t low = static_cast<uint64_t>(a2) * C::p1 + x[0];          // < p1 p2
+	const bool z = (a3 > (C::p3 - 1) / 2) || ((a3 == (C::p3 - 1) / 2) && (low > P12 / 2));
+	const uint64_t U = (low << dup) + static_cast<uint64_t>(K.r[dup]) * a3 + K.h + (z ? K.b - K.mr[dup] : 0u);
+	uint64_t rv;
+	const uint64_t qv = divb64(U + static_cast<uint64_t>(c) + K.kb, K.b, K.binv, rv);
+	c = static_cast<int64_t>(qv + K.q[dup] * a3 - (z ? K.mq[dup] + 1 : 0) - K.k);
+	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
+}
+
+// Balanced digit of s (|s| < 2^56) and carry floor((s + b/2) / b).
+__device__ __forceinline__ int32_t carry_small(int64_t s, const CarryK &K, int64_t &c)
+{
+	uint64_t rv;
+	const uint64_t qv = divb64(static_cast<uint64_t>(s) + K.h + K.kb, K.b, K.binv, rv);
+	c = static_cast<int64_t>(qv - K.k);
+	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
 }
 
 }  // namespace gfc

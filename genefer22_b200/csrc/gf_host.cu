@@ -169,10 +169,31 @@ int choose_set(uint32_t b, int n)
 	return -1;
 }
 
+// Constants of the fused CRT + carry (gf_arith.cuh, CarryK) for base b.
+CarryK carry_constants(uint32_t b, int set)
+{
+	const u128 T = (set == 0) ? u128(PrimeSet<0>::p[0]) : u128(PrimeSet<1>::p[0]) * PrimeSet<1>::p[1];
+	const u128 M = (set == 0) ? u128(PrimeSet<0>::p[0]) * PrimeSet<0>::p[1]
+							  : u128(PrimeSet<1>::p[0]) * PrimeSet<1>::p[1] * PrimeSet<1>::p[2];
+	CarryK k{};
+	k.b = b;
+	k.h = b / 2;
+	k.binv = ~uint64_t(0) / b;
+	k.k = ((uint64_t(1) << 56) + b - 1) / b;
+	k.kb = k.k * b;
+	for (int f = 1; f <= 2; ++f)
+	{
+		k.q[f - 1] = static_cast<uint64_t>((f * T) / b);
+		k.r[f - 1] = static_cast<uint32_t>((f * T) % b);
+		k.mq[f - 1] = static_cast<uint64_t>((f * M) / b);   // modulo 2^64
+		k.mr[f - 1] = static_cast<uint32_t>((f * M) % b);
+	}
+	return k;
+}
+
 // ------------------------------------------------------------------ launch dispatch
 
-constexpr int small_threads(int logn) { return (logn <= 12) ? (1 << (logn - 4)) : 512; }
-constexpr int ROW_THREADS = 256, COL_THREADS = 256, FIX_THREADS = 256;
+constexpr int FIX_THREADS = 256;
 
 template <class K>
 void set_smem(K kernel, size_t smem)
@@ -184,10 +205,9 @@ void set_smem(K kernel, size_t smem)
 template <int SET, int LOGN>
 void small_t(const Args &a, int grid, cudaStream_t s, bool prep)
 {
-	constexpr int T = small_threads(LOGN);
-	constexpr size_t smem = PrimeSet<SET>::W * ((1u << LOGN) + (1u << LOGN) / 32) * 4 + T * 8;
-	if (prep) { set_smem(k_small<SET, LOGN, T>, smem); return; }
-	k_small<SET, LOGN, T><<<grid, T, smem, s>>>(a);
+	using S = SmallShape<SET, LOGN>;
+	if (prep) { set_smem(k_small<SET, LOGN>, S::SMEM); return; }
+	k_small<SET, LOGN><<<grid, S::T, S::SMEM, s>>>(a);
 	after_launch();
 }
 
@@ -205,81 +225,75 @@ void small_set(int logn, const Args &a, int grid, cudaStream_t s, bool prep)
 	}
 }
 
-void launch_small(int set, int logn, const Args &a, int grid, cudaStream_t s, bool prep)
-{
-	if (set == 0) small_set<0>(logn, a, grid, s, prep); else small_set<1>(logn, a, grid, s, prep);
-}
-
-template <int SET, int LR>
+template <int LR>
 void col_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 {
-	constexpr int R = 1 << LR, CW = col_width(LR), RS = col_stride(LR);
-	constexpr size_t smem = size_t(PrimeSet<SET>::W) * R * RS * 4;
-	if (prep) { set_smem(k_col_fwd<SET, LR>, smem); set_smem(k_col_inv<SET, LR>, smem); return; }
-	const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / CW), static_cast<unsigned>(grid_y));
-	if (inv) k_col_inv<SET, LR><<<grid, COL_THREADS, smem, s>>>(a);
-	else k_col_fwd<SET, LR><<<grid, COL_THREADS, smem, s>>>(a);
-	after_launch();
+	if constexpr (LR <= 4)
+	{
+		// R <= 16: a thread owns a column (register kernels)
+		using S = ColRegShape<LR>;
+		if (prep) { set_smem(k_colr_inv<LR>, S::SMEM); return; }
+		const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / COLR_THREADS), static_cast<unsigned>(grid_y));
+		if (inv) k_colr_inv<LR><<<grid, COLR_THREADS, S::SMEM, s>>>(a);
+		else k_colr_fwd<LR><<<grid, COLR_THREADS, 0, s>>>(a);
+		after_launch();
+	}
+	else
+	{
+		using S = ColShape<LR>;
+		if (prep) { set_smem(k_col_fwd<LR>, S::SMEM); set_smem(k_col_inv<LR>, S::SMEM); return; }
+		const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / S::CW), static_cast<unsigned>(grid_y));
+		if (inv) k_col_inv<LR><<<grid, FS_THREADS, S::SMEM, s>>>(a);
+		else k_col_fwd<LR><<<grid, FS_THREADS, S::SMEM, s>>>(a);
+		after_launch();
+	}
 }
 
-template <int SET>
-void col_set(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+void launch_col(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 {
 	switch (lr)
 	{
-		case 3: col_t<SET, 3>(inv, a, grid_y, s, prep); break;
-		case 4: col_t<SET, 4>(inv, a, grid_y, s, prep); break;
-		case 5: col_t<SET, 5>(inv, a, grid_y, s, prep); break;
-		case 6: col_t<SET, 6>(inv, a, grid_y, s, prep); break;
-		case 7: col_t<SET, 7>(inv, a, grid_y, s, prep); break;
-		case 8: col_t<SET, 8>(inv, a, grid_y, s, prep); break;
-		case 9: col_t<SET, 9>(inv, a, grid_y, s, prep); break;
-		case 10: col_t<SET, 10>(inv, a, grid_y, s, prep); break;
+		case 3: col_t<3>(inv, a, grid_y, s, prep); break;
+		case 4: col_t<4>(inv, a, grid_y, s, prep); break;
+		case 5: col_t<5>(inv, a, grid_y, s, prep); break;
+		case 6: col_t<6>(inv, a, grid_y, s, prep); break;
+		case 7: col_t<7>(inv, a, grid_y, s, prep); break;
+		case 8: col_t<8>(inv, a, grid_y, s, prep); break;
+		case 9: col_t<9>(inv, a, grid_y, s, prep); break;
+		case 10: col_t<10>(inv, a, grid_y, s, prep); break;
 		default: fail(GFC_ERR_ARG, "four-step plan needs 3 <= lr <= 10");
 	}
 }
 
-void launch_col(int set, int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
-{
-	if (set == 0) col_set<0>(lr, inv, a, grid_y, s, prep); else col_set<1>(lr, inv, a, grid_y, s, prep);
-}
-
-template <int SET, int LC>
+template <int LC>
 void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep)
 {
-	constexpr int C = 1 << LC;
-	constexpr size_t smem = size_t(PrimeSet<SET>::W) * (C + C / 32) * 4;
-	if (prep) { set_smem(k_row<SET, LC>, smem); return; }
+	using S = RowShape<LC>;
+	if (prep) { set_smem(k_row<LC>, S::SMEM); return; }
 	const dim3 grid(1u << (a.n - LC), static_cast<unsigned>(grid_y));
-	k_row<SET, LC><<<grid, ROW_THREADS, smem, s>>>(a);
+	k_row<LC><<<grid, FS_THREADS, S::SMEM, s>>>(a);
 	after_launch();
 }
 
-template <int SET>
-void row_set(int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
+void launch_row(int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
 {
 	switch (lc)
 	{
-		case 8: row_t<SET, 8>(a, grid_y, s, prep); break;
-		case 9: row_t<SET, 9>(a, grid_y, s, prep); break;
-		case 10: row_t<SET, 10>(a, grid_y, s, prep); break;
-		case 11: row_t<SET, 11>(a, grid_y, s, prep); break;
-		case 12: row_t<SET, 12>(a, grid_y, s, prep); break;
-		case 13: row_t<SET, 13>(a, grid_y, s, prep); break;
+		case 8: row_t<8>(a, grid_y, s, prep); break;
+		case 9: row_t<9>(a, grid_y, s, prep); break;
+		case 10: row_t<10>(a, grid_y, s, prep); break;
+		case 11: row_t<11>(a, grid_y, s, prep); break;
+		case 12: row_t<12>(a, grid_y, s, prep); break;
+		case 13: row_t<13>(a, grid_y, s, prep); break;
 		default: fail(GFC_ERR_ARG, "four-step plan needs 8 <= n - lr <= 13");
 	}
-}
-
-void launch_row(int set, int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
-{
-	if (set == 0) row_set<0>(lc, a, grid_y, s, prep); else row_set<1>(lc, a, grid_y, s, prep);
 }
 
 bool plan_valid(int n, int lr)
 {
 	if (lr == 0) return (n >= 10) && (n <= SMALL_MAX_LOGN);
 	const int lc = n - lr;
-	return (lr >= 3) && (lr <= 10) && (lc >= 8) && (lc <= 13) && (col_width(lr) <= (1 << lc));
+	return (lr >= 3) && (lr <= 10) && (lc >= 8) && (lc <= 13) && ((lr <= 4) || (col_width(lr) <= (1 << lc)));
 }
 
 int default_plan(int n)
@@ -314,7 +328,8 @@ struct gfc_batch
 	uint32_t *d_err = nullptr;
 	std::vector<TestDesc> h_desc;
 	std::vector<uint32_t *> ebits;
-	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };
+	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };   // tests per prime set; d_tests lists set 0 first
+	int pending = -1;             // register whose segment carries are not yet absorbed (four-step)
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
 
@@ -329,6 +344,7 @@ struct gfc_batch
 
 struct gfc_graph
 {
+	gfc_batch *batch = nullptr;
 	int device = 0;
 	cudaStream_t stream = nullptr;
 	cudaGraph_t graph = nullptr;
@@ -359,18 +375,31 @@ void no_capture(const gfc_batch &bt)
 	if (bt.capturing) fail(GFC_ERR_STATE, "call would synchronise during graph capture");
 }
 
-Args make_args(const gfc_batch &bt, int set)
+Args make_args(const gfc_batch &bt)
 {
 	Args a{};
 	a.desc = bt.d_desc;
-	a.tests = bt.d_tests + bt.offset[set];
+	a.tests = bt.d_tests;
 	a.pos = bt.d_pos;
 	a.err = bt.d_err;
-	a.tab = bt.tab->tab[set];
+	a.tab[0] = bt.tab->tab[0];
+	a.tab[1] = bt.tab->tab[1];
 	a.n = bt.n;
 	a.lr = bt.lr;
 	a.num_regs = static_cast<int>(bt.num_regs);
 	return a;
+}
+
+// Single-CTA kernels: one launch per prime set present (tests sorted by set).
+void launch_small(const gfc_batch &bt, const Args &a0, cudaStream_t s, bool prep)
+{
+	for (int set = 0; set < 2; ++set)
+	{
+		if (bt.nset[set] == 0) continue;
+		Args a = a0;
+		a.tests = bt.d_tests + bt.offset[set];
+		if (set == 0) small_set<0>(bt.n, a, bt.nset[set], s, prep); else small_set<1>(bt.n, a, bt.nset[set], s, prep);
+	}
 }
 
 // Raises shared-memory limits of the kernels the current plan uses.
@@ -378,15 +407,11 @@ void prepare_plan(gfc_batch &bt)
 {
 	Args a{};
 	a.n = bt.n;
-	for (int s = 0; s < 2; ++s)
+	if (bt.lr == 0) launch_small(bt, a, nullptr, true);
+	else
 	{
-		if (bt.nset[s] == 0) continue;
-		if (bt.lr == 0) launch_small(s, bt.n, a, 0, nullptr, true);
-		else
-		{
-			launch_col(s, bt.lr, false, a, 0, nullptr, true);
-			launch_row(s, bt.n - bt.lr, a, 0, nullptr, true);
-		}
+		launch_col(bt.lr, false, a, 0, nullptr, true);
+		launch_row(bt.n - bt.lr, a, 0, nullptr, true);
 	}
 }
 
@@ -398,41 +423,52 @@ void launch_fixup(gfc_batch &bt, const Args &a, int g)
 	after_launch();
 }
 
-// Four-step squaring / product / forward transform for the tests of one set.
-void fourstep(gfc_batch &bt, int s, const Args &a)
+// Absorbs the pending segment carries of register bt.pending (k_fixup).
+void materialize(gfc_batch &bt)
 {
-	const int g = bt.nset[s];
-	launch_col(s, bt.lr, false, a, g, bt.stream, false);
-	launch_row(s, bt.n - bt.lr, a, g, bt.stream, false);
+	if (bt.pending < 0) return;
+	Args a = make_args(bt);
+	a.dup_mode = DUP_NONE;
+	a.dst = bt.pending;
+	launch_fixup(bt, a, static_cast<int>(bt.count));
+	bt.pending = -1;
+}
+
+// Four-step squaring / product / forward transform for all tests.  The
+// column-forward kernel absorbs pending carries of its source register (and
+// writes the fixed digits back); the column-inverse kernel leaves the carries
+// of its destination pending.
+void fourstep(gfc_batch &bt, Args a)
+{
+	const int g = static_cast<int>(bt.count);
+	a.fix = (bt.pending >= 0 && bt.pending == a.src) ? 1 : 0;
+	launch_col(bt.lr, false, a, g, bt.stream, false);
+	if (a.fix) bt.pending = -1;
+	launch_row(bt.n - bt.lr, a, g, bt.stream, false);
 	if (a.op == OP_FWD) return;
-	launch_col(s, bt.lr, true, a, g, bt.stream, false);
-	launch_fixup(bt, a, g);
+	launch_col(bt.lr, true, a, g, bt.stream, false);
+	bt.pending = a.dst;
 }
 
 // count squarings of r_0 (dup_mode DUP_NONE / DUP_ALL / DUP_BITS).
 void op_square(gfc_batch &bt, int dup_mode, uint32_t count)
 {
 	if (count == 0) return;
-	for (int s = 0; s < 2; ++s)
+	if ((bt.pending >= 0) && ((bt.lr == 0) || (bt.pending != 0))) materialize(bt);
+	Args a = make_args(bt);
+	a.op = OP_SQUARE; a.dup_mode = dup_mode; a.src = 0; a.dst = 0;
+	if (bt.lr == 0)
 	{
-		if (bt.nset[s] == 0) continue;
-		Args a = make_args(bt, s);
-		a.op = OP_SQUARE; a.dup_mode = dup_mode; a.src = 0; a.dst = 0;
-		if (bt.lr == 0)
-		{
-			a.count = static_cast<int>(count);
-			launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
-		}
-		else
-		{
-			for (uint32_t j = 0; j < count; ++j)
-			{
-				a.j = (dup_mode == DUP_BITS) ? static_cast<int>(j) : 0;
-				fourstep(bt, s, a);
-			}
-		}
+		a.count = static_cast<int>(count);
+		launch_small(bt, a, bt.stream, false);
+		return;
 	}
-	if ((bt.lr != 0) && (dup_mode == DUP_BITS))
+	for (uint32_t j = 0; j < count; ++j)
+	{
+		a.j = (dup_mode == DUP_BITS) ? static_cast<int>(j) : 0;
+		fourstep(bt, a);
+	}
+	if (dup_mode == DUP_BITS)
 	{
 		const int nt = static_cast<int>(bt.count);
 		k_pos_sub<<<(nt + 255) / 256, 256, 0, bt.stream>>>(bt.d_pos, bt.d_tests, nt, static_cast<int>(count));
@@ -444,69 +480,70 @@ void op_square(gfc_batch &bt, int dup_mode, uint32_t count)
 void op_init_multiplicand(gfc_batch &bt, size_t src)
 {
 	check_reg(bt, src);
-	for (int s = 0; s < 2; ++s)
-	{
-		if (bt.nset[s] == 0) continue;
-		Args a = make_args(bt, s);
-		a.op = OP_FWD; a.dup_mode = DUP_NONE; a.src = static_cast<int>(src); a.dst = 0;
-		if (bt.lr == 0) launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
-		else fourstep(bt, s, a);
-	}
+	if (bt.lr == 0) materialize(bt);
+	Args a = make_args(bt);
+	a.op = OP_FWD; a.dup_mode = DUP_NONE; a.src = static_cast<int>(src); a.dst = 0;
+	if (bt.lr == 0) launch_small(bt, a, bt.stream, false);
+	else fourstep(bt, a);
 }
 
 // r_dst = r_0 * r_m for all tests.
 void op_mul(gfc_batch &bt, size_t dst)
 {
 	check_reg(bt, dst);
-	for (int s = 0; s < 2; ++s)
-	{
-		if (bt.nset[s] == 0) continue;
-		Args a = make_args(bt, s);
-		a.op = OP_MUL; a.dup_mode = DUP_NONE; a.src = 0; a.dst = static_cast<int>(dst);
-		if (bt.lr == 0) launch_small(s, bt.n, a, bt.nset[s], bt.stream, false);
-		else fourstep(bt, s, a);
-	}
+	if ((bt.pending >= 0) && ((bt.lr == 0) || (bt.pending != 0))) materialize(bt);
+	Args a = make_args(bt);
+	a.op = OP_MUL; a.dup_mode = DUP_NONE; a.src = 0; a.dst = static_cast<int>(dst);
+	if (bt.lr == 0) launch_small(bt, a, bt.stream, false);
+	else fourstep(bt, a);
 }
 
 // One squaring at a time with events around each kernel (see gfc_batch_time_kernels).
 void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
 {
 	no_capture(bt);
+	if ((bt.pending >= 0) && (bt.pending != 0)) materialize(bt);
 	cudaEvent_t ev[5];
 	for (auto &e : ev) GFC_CK(cudaEventCreate(&e));
 	double acc[5] = { 0, 0, 0, 0, 0 };
 	auto span = [&](int i, int j) { float t = 0; GFC_CK(cudaEventElapsedTime(&t, ev[i], ev[j])); return static_cast<double>(t); };
 	try
 	{
+		Args a = make_args(bt);
+		a.op = OP_SQUARE; a.dup_mode = DUP_NONE; a.count = 1; a.src = 0; a.dst = 0;
+		const int g = static_cast<int>(bt.count);
 		for (uint32_t r = 0; r < reps; ++r)
-			for (int s = 0; s < 2; ++s)
+		{
+			GFC_CK(cudaEventRecord(ev[0], bt.stream));
+			if (bt.lr == 0)
 			{
-				if (bt.nset[s] == 0) continue;
-				Args a = make_args(bt, s);
-				a.op = OP_SQUARE; a.dup_mode = DUP_NONE; a.count = 1; a.src = 0; a.dst = 0;
-				const int g = bt.nset[s];
-				GFC_CK(cudaEventRecord(ev[0], bt.stream));
-				if (bt.lr == 0)
-				{
-					launch_small(s, bt.n, a, g, bt.stream, false);
-					GFC_CK(cudaEventRecord(ev[1], bt.stream));
-					GFC_CK(cudaEventSynchronize(ev[1]));
-					acc[0] += span(0, 1);
-				}
-				else
-				{
-					launch_col(s, bt.lr, false, a, g, bt.stream, false);
-					GFC_CK(cudaEventRecord(ev[1], bt.stream));
-					launch_row(s, bt.n - bt.lr, a, g, bt.stream, false);
-					GFC_CK(cudaEventRecord(ev[2], bt.stream));
-					launch_col(s, bt.lr, true, a, g, bt.stream, false);
-					GFC_CK(cudaEventRecord(ev[3], bt.stream));
-					launch_fixup(bt, a, g);
-					GFC_CK(cudaEventRecord(ev[4], bt.stream));
-					GFC_CK(cudaEventSynchronize(ev[4]));
-					acc[1] += span(0, 1); acc[2] += span(1, 2); acc[3] += span(2, 3); acc[4] += span(3, 4);
-				}
+				launch_small(bt, a, bt.stream, false);
+				GFC_CK(cudaEventRecord(ev[1], bt.stream));
+				GFC_CK(cudaEventSynchronize(ev[1]));
+				acc[0] += span(0, 1);
 			}
+			else
+			{
+				a.fix = (bt.pending == 0) ? 1 : 0;
+				launch_col(bt.lr, false, a, g, bt.stream, false);
+				GFC_CK(cudaEventRecord(ev[1], bt.stream));
+				launch_row(bt.n - bt.lr, a, g, bt.stream, false);
+				GFC_CK(cudaEventRecord(ev[2], bt.stream));
+				launch_col(bt.lr, true, a, g, bt.stream, false);
+				bt.pending = 0;
+				GFC_CK(cudaEventRecord(ev[3], bt.stream));
+				GFC_CK(cudaEventSynchronize(ev[3]));
+				acc[1] += span(0, 1); acc[2] += span(1, 2); acc[3] += span(2, 3);
+			}
+		}
+		if (bt.lr != 0)
+		{
+			GFC_CK(cudaEventRecord(ev[3], bt.stream));
+			materialize(bt);
+			GFC_CK(cudaEventRecord(ev[4], bt.stream));
+			GFC_CK(cudaEventSynchronize(ev[4]));
+			acc[4] = span(3, 4) * reps;   // one stand-alone fix-up, for reference
+		}
 	}
 	catch (...)
 	{
@@ -517,17 +554,13 @@ void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
 	for (int i = 0; i < 5; ++i) ms[i] = static_cast<float>(acc[i] / (reps ? reps : 1));
 }
 
-Args all_args(const gfc_batch &bt)
-{
-	Args a = make_args(bt, 0);
-	a.tests = bt.d_tests;
-	return a;
-}
+Args all_args(const gfc_batch &bt) { return make_args(bt); }
 
 void op_set(gfc_batch &bt, uint32_t value)
 {
 	for (size_t i = 0; i < bt.count; ++i)
 		if (value > bt.b[i] / 2) fail(GFC_ERR_ARG, "set: value must be <= b/2");
+	if (bt.pending == 0) bt.pending = -1;     // register 0 is overwritten
 	Args a = all_args(bt);
 	a.dst = 0;
 	const dim3 grid(static_cast<unsigned>((bt.N + 255) / 256 < 1024 ? (bt.N + 255) / 256 : 1024), static_cast<unsigned>(bt.count));
@@ -539,6 +572,8 @@ void op_copy(gfc_batch &bt, size_t dst, size_t src)
 {
 	check_reg(bt, dst); check_reg(bt, src);
 	if (dst == src) return;
+	if (bt.pending == static_cast<int>(src)) materialize(bt);
+	else if (bt.pending == static_cast<int>(dst)) bt.pending = -1;   // overwritten
 	Args a = all_args(bt);
 	a.dst = static_cast<int>(dst); a.src = static_cast<int>(src);
 	const size_t n4 = bt.N / 4;
@@ -628,8 +663,8 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 		d.carry = bt->carry + i * (N / SEG);
 		d.ebits = nullptr;
 		d.b = b[i];
-		d.binv = ~uint64_t(0) / b[i];
 		d.set = bt->set[i];
+		d.ck = carry_constants(b[i], bt->set[i]);
 	}
 	GFC_CK(cudaMemcpyAsync(bt->d_desc, bt->h_desc.data(), count * sizeof(TestDesc), cudaMemcpyHostToDevice, bt->stream));
 	GFC_CK(cudaMemcpyAsync(bt->d_tests, tests.data(), count * sizeof(int32_t), cudaMemcpyHostToDevice, bt->stream));
@@ -744,6 +779,7 @@ GFC_API int gfc_save_context(gfc_transform *t, void *buf, size_t size, size_t nu
 		cudaSetDevice(t->device);
 		const uint32_t kind = GFC_CONTEXT_KIND;
 		std::memcpy(buf, &kind, sizeof(kind));
+		materialize(*t);
 		GFC_CK(cudaMemcpyAsync(static_cast<char *>(buf) + sizeof(kind), t->regs, num_regs * t->N * sizeof(int32_t),
 							   cudaMemcpyDeviceToHost, t->stream));
 		op_sync(*t);
@@ -763,6 +799,7 @@ GFC_API int gfc_read_context(gfc_transform *t, const void *buf, size_t size, siz
 		for (size_t r = 0; r < num_regs; ++r) check_digits(*t, 0, d + r * t->N);
 		no_capture(*t);
 		cudaSetDevice(t->device);
+		materialize(*t);
 		GFC_CK(cudaMemcpyAsync(t->regs, d, num_regs * t->N * sizeof(int32_t), cudaMemcpyHostToDevice, t->stream));
 		op_sync(*t);
 	});
@@ -886,6 +923,7 @@ GFC_API int gfc_batch_get_zi(gfc_batch *bt, size_t test, size_t reg, int32_t *ou
 		check_test(*bt, test); check_reg(*bt, reg);
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
+		materialize(*bt);
 		GFC_CK(cudaMemcpyAsync(out, reg_ptr(*bt, test, reg), bt->N * sizeof(int32_t), cudaMemcpyDeviceToHost, bt->stream));
 		op_sync(*bt);
 	});
@@ -899,6 +937,7 @@ GFC_API int gfc_batch_set_zi(gfc_batch *bt, size_t test, size_t reg, const int32
 		check_digits(*bt, test, in);
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
+		materialize(*bt);
 		GFC_CK(cudaMemcpyAsync(reg_ptr(*bt, test, reg), in, bt->N * sizeof(int32_t), cudaMemcpyHostToDevice, bt->stream));
 		GFC_CK(cudaStreamSynchronize(bt->stream));
 	});
@@ -911,6 +950,7 @@ GFC_API int gfc_batch_get_all(gfc_batch *bt, size_t reg, int32_t *out)
 		check_reg(*bt, reg);
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
+		materialize(*bt);
 		// registers of one test are contiguous: reg r of test i at (i * num_regs + r) * N
 		GFC_CK(cudaMemcpy2DAsync(out, bt->N * sizeof(int32_t), reg_ptr(*bt, 0, reg), bt->num_regs * bt->N * sizeof(int32_t),
 								 bt->N * sizeof(int32_t), bt->count, cudaMemcpyDeviceToHost, bt->stream));
@@ -926,6 +966,7 @@ GFC_API int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in)
 		for (size_t i = 0; i < bt->count; ++i) check_digits(*bt, i, in + i * bt->N);
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
+		materialize(*bt);
 		GFC_CK(cudaMemcpy2DAsync(reg_ptr(*bt, 0, reg), bt->num_regs * bt->N * sizeof(int32_t), in, bt->N * sizeof(int32_t),
 								 bt->N * sizeof(int32_t), bt->count, cudaMemcpyHostToDevice, bt->stream));
 		GFC_CK(cudaStreamSynchronize(bt->stream));
@@ -939,6 +980,7 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 		if (!plan_valid(bt->n, lr)) fail(GFC_ERR_ARG, "set_plan: invalid plan for this n");
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
+		materialize(*bt);
 		GFC_CK(cudaStreamSynchronize(bt->stream));
 		bt->lr = lr;
 		prepare_plan(*bt);
@@ -973,6 +1015,7 @@ GFC_API int gfc_batch_capture_begin(gfc_batch *bt)
 		GFC_NULLCHK(bt);
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
+		materialize(*bt);   // a graph starts and ends with every register materialised
 		GFC_CK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
 		bt->capturing = true;
 		bt->capture_start = g_launches.load();
@@ -986,9 +1029,10 @@ GFC_API int gfc_batch_capture_end(gfc_batch *bt, gfc_graph **out)
 		*out = nullptr;
 		if (!bt->capturing) fail(GFC_ERR_STATE, "capture_end without capture_begin");
 		cudaSetDevice(bt->device);
+		try { materialize(*bt); } catch (...) { }
 		bt->capturing = false;
 		std::unique_ptr<gfc_graph> g(new gfc_graph());
-		g->device = bt->device; g->stream = bt->stream;
+		g->batch = bt; g->device = bt->device; g->stream = bt->stream;
 		// recorded launches are counted when the graph runs, not here
 		g->kernels = g_launches.load() - bt->capture_start;
 		g_launches.fetch_sub(g->kernels);
@@ -1003,6 +1047,7 @@ GFC_API int gfc_graph_launch(gfc_graph *g)
 	return guard([&] {
 		GFC_NULLCHK(g);
 		cudaSetDevice(g->device);
+		if (g->batch != nullptr) materialize(*g->batch);
 		GFC_CK(cudaGraphLaunch(g->exec, g->stream));
 		g_launches.fetch_add(g->kernels);
 	});

@@ -14,6 +14,9 @@
 //     on column tiles, k_row the remaining stages + pointwise + inverse on
 //     rows, k_col_inv the last inverse stages, CRT and the carry inside
 //     16-digit segments, and k_fixup adds each segment's carry to the next.
+// Every kernel serves all tests of a batch in one launch; each CTA picks the
+// code path of its test's prime set (W = 2 or 3) and processes the W planes
+// of a radix group together.
 #pragma once
 
 #include <type_traits>
@@ -23,9 +26,11 @@ namespace gfc {
 
 enum : int { OP_SQUARE = 0, OP_MUL = 1, OP_FWD = 2 };
 enum : int { DUP_NONE = 0, DUP_ALL = 1, DUP_BITS = 2 };
+enum : int { PM_FWD = 0, PM_INV = 1, PM_MID_SQ = 2, PM_MID_MUL = 3 };
 
 constexpr int SEG = 16;          // digits per carry segment
 constexpr int SMALL_MAX_LOGN = 14;
+constexpr int WMAX = 3;
 
 struct TestDesc
 {
@@ -34,7 +39,7 @@ struct TestDesc
 	uint32_t *zp;           // 3 x N multiplicand (transform domain, normal form)
 	int64_t *carry;         // N / SEG segment carries
 	const uint32_t *ebits;  // exponent bits, bit i in word i/32 (may be null)
-	uint64_t binv;          // floor((2^64 - 1) / b)
+	CarryK ck;              // constants of the fused CRT + carry for this b
 	uint32_t b;
 	int32_t set;            // prime set: 0 (W = 2), 1 (W = 3)
 };
@@ -51,10 +56,11 @@ struct Args
 	const int32_t *tests;   // indices of the tests this launch serves
 	int64_t *pos;           // per-test current exponent bit index
 	uint32_t *err;          // error flags (bit 0: carry not absorbed)
-	Tables tab;
+	Tables tab[2];          // root tables of prime set 0 and 1
 	int n, lr;              // log2 N, log2 R (four-step)
 	int num_regs, src, dst; // registers
 	int op, dup_mode, count, j;  // operation, dup source, squarings (k_small), squaring index in block
+	int fix;                // four-step column-forward: register src has pending segment carries
 };
 
 template <int SET, int PL>
@@ -66,6 +72,16 @@ __device__ __forceinline__ void for_planes(F &&f)
 	f(std::integral_constant<int, 0>{});
 	f(std::integral_constant<int, 1>{});
 	if constexpr (PrimeSet<SET>::W == 3) f(std::integral_constant<int, 2>{});
+}
+
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f)
+{
+	if constexpr (B < E)
+	{
+		f(std::integral_constant<int, B>{});
+		static_for<B + 1, E>(f);
+	}
 }
 
 __device__ __forceinline__ bool exp_bit(const uint32_t *ebits, int64_t i)
@@ -89,20 +105,22 @@ __device__ __forceinline__ bool get_dup(const Args &a, const TestDesc &d, int t,
 
 // Adds carry `c` to the digits of one segment: reduces while |c| > 1, then
 // leaves the last +-1 in the next digit unreduced (|digit| <= b/2 + 1).
+// `touched` receives the number of leading digits that changed; returns
+// false if the carry did not fit in the segment.
 template <int D>
-__device__ __forceinline__ bool absorb(int32_t (&dg)[D], int64_t c, uint32_t b, uint64_t binv)
+__device__ __forceinline__ bool absorb(int32_t (&dg)[D], int64_t c, const CarryK &K, int &touched)
 {
 	bool active = (c != 0);
+	touched = 0;
 #pragma unroll
 	for (int k = 0; k < D; ++k)
 	{
 		if (active)
 		{
+			touched = k + 1;
 			if ((c > 1) || (c < -1))
 			{
-				int64_t q;
-				dg[k] = digit_carry64(static_cast<int64_t>(dg[k]) + c, b, binv, q);
-				c = q;
+				dg[k] = carry_small(static_cast<int64_t>(dg[k]) + c, K, c);
 			}
 			else
 			{
@@ -114,198 +132,169 @@ __device__ __forceinline__ bool absorb(int32_t (&dg)[D], int64_t c, uint32_t b, 
 	return !active;
 }
 
+template <int D>
+__device__ __forceinline__ bool absorb(int32_t (&dg)[D], int64_t c, const CarryK &K)
+{
+	int touched;
+	return absorb<D>(dg, c, K, touched);
+}
+
+// Carry into segment s (16 digits) of a register with N / SEG segments.
+__device__ __forceinline__ int64_t carry_in(const TestDesc &d, size_t s, size_t nseg)
+{
+	return (s == 0) ? -d.carry[nseg - 1] : d.carry[s - 1];
+}
+
+// Absorbs the pending carry of one segment held in shared memory (element i
+// of the segment at seg[i * istride]) and writes the touched digits back to
+// the register in global memory at g.
+__device__ __forceinline__ void fix_segment(const TestDesc &d, int32_t *seg, int istride, int32_t *g, int64_t cin,
+											uint32_t *err)
+{
+	if (cin == 0) return;
+	int32_t dg[SEG];
+#pragma unroll
+	for (int i = 0; i < SEG; ++i) dg[i] = seg[i * istride];
+	int touched;
+	if (!absorb<SEG>(dg, cin, d.ck, touched)) atomicOr(err, 1u);
+#pragma unroll
+	for (int i = 0; i < SEG; ++i)
+		if (i < touched) { seg[i * istride] = dg[i]; g[i] = dg[i]; }
+}
+
+// Radix schedule of a length-2^L transform: passes of 4 stages starting at
+// stage 4p; the last pass takes the remainder.
+template <int L>
+struct Sched
+{
+	static constexpr int NP = (L + 3) / 4;
+	__host__ __device__ static constexpr int r(int p) { return (p < L / 4) ? 4 : (L % 4); }
+};
+
 // ------------------------------------------------------------------ passes
 
-template <int SET, int PL, int r, class Map>
-__device__ __forceinline__ void pass_fwd(uint32_t *buf, const Map &mp, int l, int sigma, int lanes_log, bool lane_fast,
-										 uint32_t base0, uint32_t base_step, const uint32_t *__restrict__ tw)
+// One radix-2^r pass over the W planes (pstride words apart) of a shared-memory
+// tile holding 2^lanes_log transforms of length 2^l.  Work item = one group of
+// one lane, all planes.  PM_FWD / PM_INV: r forward / inverse stages;
+// PM_MID_SQ / PM_MID_MUL: r forward stages, pointwise square (or product with
+// the multiplicand at zrow[PL * zstride + (lane << l) + i]), r inverse stages.
+template <int SET, int r, int MODE, int L, int SIGMA, class Map>
+__device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
+										 uint32_t base_step, const Tables &tab, const uint32_t *__restrict__ zrow,
+										 size_t zstride)
 {
-	using Z = ZS<SET, PL>;
-	const int groups_log = l - r;
-	const int items = 1 << (lanes_log + groups_log);
+	constexpr int W = PrimeSet<SET>::W;
+	constexpr int E = 1 << r;
+	constexpr int GL = L - r;                 // log2 groups per transform
+	constexpr int STEP = 1 << (L - SIGMA - r);
+	const int items = 1 << (lanes_log + GL);
 	for (int it = threadIdx.x; it < items; it += blockDim.x)
 	{
 		int lane, g;
 		if (lane_fast) { lane = it & ((1 << lanes_log) - 1); g = it >> lanes_log; }
-		else { g = it & ((1 << groups_log) - 1); lane = it >> groups_log; }
-		const Group G(g, l, sigma, r);
-		uint32_t x[1 << r];
+		else { g = it & ((1 << GL) - 1); lane = it >> GL; }
+		const Group G(g, L, SIGMA, r);
+		const uint32_t tb = ((base0 + static_cast<uint32_t>(lane) * base_step) << SIGMA) + G.blk;
+		const int base = Map::addr(G.i0, lane);
+#pragma unroll 1
+		for (int pl = 0; pl < W; ++pl)
+		{
+			const auto z = prime_rt<SET>(pl);
+			uint32_t *pb = buf + pl * pstride + base;
+			uint32_t x[E];
 #pragma unroll
-		for (int m = 0; m < (1 << r); ++m) x[m] = buf[mp(G.i0 + m * G.step, lane)];
-		const uint32_t base = base0 + static_cast<uint32_t>(lane) * base_step;
-		fwd_reg<Z, r>(x, (base << sigma) + G.blk, tw);
+			for (int m = 0; m < E; ++m) x[m] = pb[Map::off(m, STEP)];
+			if constexpr (MODE != PM_INV) fwd_reg<decltype(z), r>(z, x, tb, tab.fw[pl]);
+			if constexpr (MODE == PM_MID_SQ)
+			{
 #pragma unroll
-		for (int m = 0; m < (1 << r); ++m) buf[mp(G.i0 + m * G.step, lane)] = x[m];
+				for (int m = 0; m < E; ++m) x[m] = z.mul(x[m], x[m]);
+			}
+			if constexpr (MODE == PM_MID_MUL)
+			{
+				const uint32_t *zz = zrow + pl * zstride + (static_cast<size_t>(lane) << L) + G.i0;
+#pragma unroll
+				for (int m = 0; m < E; ++m) x[m] = z.mul(x[m], __ldg(&zz[m * STEP]));
+			}
+			if constexpr (MODE != PM_FWD)
+				inv_reg<decltype(z), r>(z, x, tb, tab.iv[pl], tb == 1u, __ldg(&tab.fw[pl][0]), __ldg(&tab.iv[pl][0]));
+#pragma unroll
+			for (int m = 0; m < E; ++m) pb[Map::off(m, STEP)] = x[m];
+		}
 	}
 }
 
-template <int SET, int PL, int r, class Map>
-__device__ __forceinline__ void pass_inv(uint32_t *buf, const Map &mp, int l, int sigma, int lanes_log, bool lane_fast,
-										 uint32_t base0, uint32_t base_step, const uint32_t *__restrict__ tw,
-										 const uint32_t *__restrict__ twi)
+// Forward passes 0 .. NP-1 (or NP-2 with SKIP_LAST), a barrier after each.
+template <int SET, int L, bool SKIP_LAST, class Map>
+__device__ __forceinline__ void run_fwd(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
+										uint32_t base_step, const Tables &tab)
 {
-	using Z = ZS<SET, PL>;
-	const int groups_log = l - r;
-	const int items = 1 << (lanes_log + groups_log);
-	const uint32_t c_norm = __ldg(&tw[0]), k_norm = __ldg(&twi[0]);
-	for (int it = threadIdx.x; it < items; it += blockDim.x)
-	{
-		int lane, g;
-		if (lane_fast) { lane = it & ((1 << lanes_log) - 1); g = it >> lanes_log; }
-		else { g = it & ((1 << groups_log) - 1); lane = it >> groups_log; }
-		const Group G(g, l, sigma, r);
-		uint32_t x[1 << r];
-#pragma unroll
-		for (int m = 0; m < (1 << r); ++m) x[m] = buf[mp(G.i0 + m * G.step, lane)];
-		const uint32_t base = base0 + static_cast<uint32_t>(lane) * base_step;
-		const uint32_t tb = (base << sigma) + G.blk;
-		inv_reg<Z, r>(x, tb, twi, tb == 1u, c_norm, k_norm);
-#pragma unroll
-		for (int m = 0; m < (1 << r); ++m) buf[mp(G.i0 + m * G.step, lane)] = x[m];
-	}
-}
-
-// Last forward pass + pointwise square (or product with the multiplicand) +
-// first inverse pass, without leaving registers.  `zrow` points at the
-// multiplicand plane at this tile's first element (row layout only).
-template <int SET, int PL, int r, class Map>
-__device__ __forceinline__ void pass_mid(uint32_t *buf, const Map &mp, int l, int sigma, int lanes_log,
-										 uint32_t base0, uint32_t base_step, const uint32_t *__restrict__ tw,
-										 const uint32_t *__restrict__ twi, const uint32_t *__restrict__ zrow, bool is_mul)
-{
-	using Z = ZS<SET, PL>;
-	const int groups_log = l - r;
-	const int items = 1 << (lanes_log + groups_log);
-	const uint32_t c_norm = __ldg(&tw[0]), k_norm = __ldg(&twi[0]);
-	for (int it = threadIdx.x; it < items; it += blockDim.x)
-	{
-		const int g = it & ((1 << groups_log) - 1), lane = it >> groups_log;
-		const Group G(g, l, sigma, r);
-		uint32_t x[1 << r];
-#pragma unroll
-		for (int m = 0; m < (1 << r); ++m) x[m] = buf[mp(G.i0 + m * G.step, lane)];
-		const uint32_t base = base0 + static_cast<uint32_t>(lane) * base_step;
-		const uint32_t tb = (base << sigma) + G.blk;
-		fwd_reg<Z, r>(x, tb, tw);
-		if (is_mul)
-		{
-#pragma unroll
-			for (int m = 0; m < (1 << r); ++m) x[m] = Z::mul(x[m], __ldg(&zrow[(lane << l) + G.i0 + m * G.step]));
-		}
-		else
-		{
-#pragma unroll
-			for (int m = 0; m < (1 << r); ++m) x[m] = Z::mul(x[m], x[m]);
-		}
-		inv_reg<Z, r>(x, tb, twi, tb == 1u, c_norm, k_norm);
-#pragma unroll
-		for (int m = 0; m < (1 << r); ++m) buf[mp(G.i0 + m * G.step, lane)] = x[m];
-	}
-}
-
-// Radix schedule: passes of 4 stages, the last one takes the remainder.
-__host__ __device__ constexpr int num_passes(int l) { return (l + 3) / 4; }
-__host__ __device__ constexpr int pass_r(int l, int p) { return (p < l / 4) ? 4 : (l % 4); }
-
-template <int SET, int PL, class Map>
-__device__ __forceinline__ void run_fwd(uint32_t *buf, const Map &mp, int l, int lanes_log, bool lane_fast, uint32_t base0,
-										uint32_t base_step, const uint32_t *tw, int npass)
-{
-	int sigma = 0;
-	for (int p = 0; p < npass; ++p)
-	{
-		const int r = pass_r(l, p);
-		switch (r)
-		{
-			case 4: pass_fwd<SET, PL, 4>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw); break;
-			case 3: pass_fwd<SET, PL, 3>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw); break;
-			case 2: pass_fwd<SET, PL, 2>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw); break;
-			default: pass_fwd<SET, PL, 1>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw); break;
-		}
-		sigma += r;
+	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
+	static_for<0, NP>([&](auto P) {
+		constexpr int p = decltype(P)::value;
+		pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
+															  nullptr, 0);
 		__syncthreads();
-	}
+	});
 }
 
-// Inverse passes p = npass-1 .. 0 (stages in reverse order).
-template <int SET, int PL, class Map>
-__device__ __forceinline__ void run_inv(uint32_t *buf, const Map &mp, int l, int lanes_log, bool lane_fast, uint32_t base0,
-										uint32_t base_step, const uint32_t *tw, const uint32_t *twi, int npass)
+// Inverse passes NP-1 (or NP-2 with SKIP_LAST) .. 0.
+template <int SET, int L, bool SKIP_LAST, class Map>
+__device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
+										uint32_t base_step, const Tables &tab)
 {
-	int sigma = 0;
-	for (int p = 0; p < npass; ++p) sigma += pass_r(l, p);
-	for (int p = npass - 1; p >= 0; --p)
-	{
-		const int r = pass_r(l, p);
-		sigma -= r;
-		switch (r)
-		{
-			case 4: pass_inv<SET, PL, 4>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw, twi); break;
-			case 3: pass_inv<SET, PL, 3>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw, twi); break;
-			case 2: pass_inv<SET, PL, 2>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw, twi); break;
-			default: pass_inv<SET, PL, 1>(buf, mp, l, sigma, lanes_log, lane_fast, base0, base_step, tw, twi); break;
-		}
+	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
+	static_for<0, NP>([&](auto Q) {
+		constexpr int p = NP - 1 - decltype(Q)::value;
+		pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
+															  nullptr, 0);
 		__syncthreads();
-	}
+	});
 }
 
-// Full squaring/product core on `lanes` row transforms of length 2^l held in
-// shared memory: forward, pointwise, inverse.
-template <int SET, int PL>
-__device__ __forceinline__ void row_core(uint32_t *buf, const RowMap &mp, int l, int lanes_log, uint32_t base0,
-										 const uint32_t *tw, const uint32_t *twi, const uint32_t *zrow, int op)
+// Row transforms in shared memory: forward (OP_FWD), or forward + pointwise
+// square / product + inverse.
+template <int SET, int L, class Map>
+__device__ __forceinline__ void row_core(uint32_t *buf, int pstride, int lanes_log, uint32_t base0, const Tables &tab,
+										 const uint32_t *zrow, size_t zstride, int op)
 {
-	const int np = num_passes(l);
-	if (op == OP_FWD) { run_fwd<SET, PL>(buf, mp, l, lanes_log, false, base0, 1u, tw, np); return; }
-	run_fwd<SET, PL>(buf, mp, l, lanes_log, false, base0, 1u, tw, np - 1);
-	int sigma = 0;
-	for (int p = 0; p < np - 1; ++p) sigma += pass_r(l, p);
-	const int r = pass_r(l, np - 1);
-	const bool is_mul = (op == OP_MUL);
-	switch (r)
-	{
-		case 4: pass_mid<SET, PL, 4>(buf, mp, l, sigma, lanes_log, base0, 1u, tw, twi, zrow, is_mul); break;
-		case 3: pass_mid<SET, PL, 3>(buf, mp, l, sigma, lanes_log, base0, 1u, tw, twi, zrow, is_mul); break;
-		case 2: pass_mid<SET, PL, 2>(buf, mp, l, sigma, lanes_log, base0, 1u, tw, twi, zrow, is_mul); break;
-		default: pass_mid<SET, PL, 1>(buf, mp, l, sigma, lanes_log, base0, 1u, tw, twi, zrow, is_mul); break;
-	}
+	constexpr int PL = Sched<L>::NP - 1;
+	if (op == OP_FWD) { run_fwd<SET, L, false, Map>(buf, pstride, lanes_log, false, base0, 1u, tab); return; }
+	run_fwd<SET, L, true, Map>(buf, pstride, lanes_log, false, base0, 1u, tab);
+	if (op == OP_MUL)
+		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map>(buf, pstride, lanes_log, false, base0, 1u, tab, zrow, zstride);
+	else
+		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map>(buf, pstride, lanes_log, false, base0, 1u, tab, zrow, zstride);
 	__syncthreads();
-	// remaining inverse passes np-2 .. 0
-	for (int p = np - 2; p >= 0; --p)
-	{
-		const int rr = pass_r(l, p);
-		sigma -= rr;
-		switch (rr)
-		{
-			case 4: pass_inv<SET, PL, 4>(buf, mp, l, sigma, lanes_log, false, base0, 1u, tw, twi); break;
-			case 3: pass_inv<SET, PL, 3>(buf, mp, l, sigma, lanes_log, false, base0, 1u, tw, twi); break;
-			case 2: pass_inv<SET, PL, 2>(buf, mp, l, sigma, lanes_log, false, base0, 1u, tw, twi); break;
-			default: pass_inv<SET, PL, 1>(buf, mp, l, sigma, lanes_log, false, base0, 1u, tw, twi); break;
-		}
-		__syncthreads();
-	}
+	run_inv<SET, L, true, Map>(buf, pstride, lanes_log, false, base0, 1u, tab);
 }
 
 // ------------------------------------------------------------------ k_small
 
-// Shared memory: W planes of N (+N/32 padding) words, then T int64 carries.
-template <int SET, int LOGN, int T>
-__global__ void __launch_bounds__(T, 1) k_small(const Args a)
+// Single-CTA shape for one prime set: T threads, D = N / T digits each;
+// MINB CTAs per SM bound the register budget.
+template <int SET, int LOGN>
+struct SmallShape
 {
-	constexpr int W = PrimeSet<SET>::W;
-	constexpr int N = 1 << LOGN;
-	constexpr int D = N / T;           // digits per thread (multiple of SEG)
-	constexpr int PN = N + N / 32;
-	static_assert(D % SEG == 0, "digits per thread");
-	extern __shared__ __align__(16) uint32_t sm[];
-	int64_t *const sc = reinterpret_cast<int64_t *>(sm + W * PN);
+	static constexpr int W = PrimeSet<SET>::W;
+	static constexpr int N = 1 << LOGN;
+	static constexpr int PN = N + N / 32;                 // padded plane
+	static constexpr int T = (LOGN <= 12) ? (N / 16) : 512;
+	static constexpr int MINB = (T <= 128) ? 4 : ((T == 256) ? 2 : 1);
+	static constexpr size_t SMEM = size_t(W) * PN * 4 + size_t(T) * 8;
+};
 
-	const int t = a.tests[blockIdx.x];
-	const TestDesc &d = a.desc[t];
+template <int SET, int LOGN>
+__device__ __forceinline__ void small_body(const Args &a, int t, const TestDesc &d, uint32_t *sm)
+{
+	using S = SmallShape<SET, LOGN>;
+	constexpr int N = S::N, PN = S::PN, T = S::T;
+	constexpr int D = N / T;           // digits per thread (multiple of SEG)
+	static_assert(D % SEG == 0, "digits per thread");
+	int64_t *const sc = reinterpret_cast<int64_t *>(sm + S::W * PN);
+	const Tables &tab = a.tab[SET];
 	const int tid = threadIdx.x;
-	const uint32_t b = d.b;
-	const uint64_t binv = d.binv;
-	const RowMap mp{LOGN};
+	using MP = RowMap<LOGN>;
 
 	int32_t dg[D];
 	{
@@ -322,32 +311,25 @@ __global__ void __launch_bounds__(T, 1) k_small(const Args a)
 	int done = 0;
 	for (int it = 0; it < iters; ++it)
 	{
-		bool active;
-		const bool dup = (a.op == OP_SQUARE) ? get_dup(a, d, t, it, active) : (active = true, false);
+		bool active = true;
+		const bool dup = (a.op == OP_SQUARE) ? get_dup(a, d, t, it, active) : false;
 		if (!active) break;
 
 		for_planes<SET>([&](auto PLc) {
 			constexpr int PL = decltype(PLc)::value;
 			using Z = ZS<SET, PL>;
-			uint32_t *pl = sm + PL * PN;
 #pragma unroll
-			for (int i = 0; i < D; ++i) pl[mp(tid * D + i, 0)] = Z::from_int(dg[i]);
+			for (int i = 0; i < D; ++i) sm[PL * PN + MP::addr(tid * D + i, 0)] = Z::from_int(dg[i]);
 		});
 		__syncthreads();
 
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			row_core<SET, PL>(sm + PL * PN, mp, LOGN, 0, 1u, a.tab.fw[PL], a.tab.iv[PL], d.zp + PL * N, a.op);
-		});
+		row_core<SET, LOGN, MP>(sm, PN, 0, 1u, tab, d.zp, N, a.op);
 
 		if (a.op == OP_FWD)
 		{
-			for_planes<SET>([&](auto PLc) {
-				constexpr int PL = decltype(PLc)::value;
-				const uint32_t *pl = sm + PL * PN;
-				uint32_t *zo = d.zp + PL * N;
-				for (int i = tid; i < N; i += T) zo[i] = pl[mp(i, 0)];
-			});
+#pragma unroll
+			for (int pl = 0; pl < PrimeSet<SET>::W; ++pl)
+				for (int i = tid; i < N; i += T) d.zp[pl * N + i] = sm[pl * PN + MP::addr(i, 0)];
 			return;
 		}
 
@@ -357,18 +339,14 @@ __global__ void __launch_bounds__(T, 1) k_small(const Args a)
 		for (int i = 0; i < D; ++i)
 		{
 			uint32_t x[3];
-			for_planes<SET>([&](auto PLc) {
-				constexpr int PL = decltype(PLc)::value;
-				x[PL] = sm[PL * PN + mp(tid * D + i, 0)];
-			});
-			i128 v = crt<SET>(x);
-			if (dup) v += v;
-			dg[i] = digit_carry(v + c, b, binv, c);
+#pragma unroll
+			for (int pl = 0; pl < PrimeSet<SET>::W; ++pl) x[pl] = sm[pl * PN + MP::addr(tid * D + i, 0)];
+			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
 		}
 		sc[tid] = c;
 		__syncthreads();
 		const int64_t cin = (tid == 0) ? -sc[T - 1] : sc[tid - 1];
-		if (!absorb<D>(dg, cin, b, binv)) atomicOr(a.err, 1u);
+		if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
 		__syncthreads();
 		++done;
 	}
@@ -381,126 +359,174 @@ __global__ void __launch_bounds__(T, 1) k_small(const Args a)
 	if ((tid == 0) && (a.op == OP_SQUARE) && (a.dup_mode == DUP_BITS)) a.pos[t] -= done;
 }
 
+// One CTA per test of prime set SET; shared memory SmallShape<SET, LOGN>::SMEM.
+template <int SET, int LOGN>
+__global__ void __launch_bounds__(SmallShape<SET, LOGN>::T, SmallShape<SET, LOGN>::MINB) k_small(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.x];
+	small_body<SET, LOGN>(a, t, a.desc[t], sm);
+}
+
 // ------------------------------------------------------------------ four-step
 
+__host__ __device__ constexpr int ilog2c(int x) { return (x <= 1) ? 0 : 1 + ilog2c(x / 2); }
 __host__ __device__ constexpr int col_width(int lr) { return (lr >= 10) ? 16 : ((4096 >> lr) > 32 ? (4096 >> lr) : 32); }
-__host__ __device__ constexpr int col_stride(int lr) { return (col_width(lr) == 16) ? 17 : col_width(lr); }
 
-// Columns: tile of cw columns x R rows; first log2 R forward stages.
-template <int SET, int LR>
-__global__ void __launch_bounds__(256) k_col_fwd(const Args a)
+// Column tile: CW columns x R rows per plane, row stride RS (ColMap padding).
+template <int LR>
+struct ColShape
 {
-	constexpr int R = 1 << LR, CW = col_width(LR), RS = col_stride(LR);
-	constexpr int CWL = (CW == 16) ? 4 : ((CW == 32) ? 5 : ((CW == 64) ? 6 : ((CW == 128) ? 7 : ((CW == 256) ? 8 : 9))));
-	extern __shared__ __align__(16) uint32_t sm[];
-	const int t = a.tests[blockIdx.y];
-	const TestDesc &d = a.desc[t];
-	bool active;
-	(void)get_dup(a, d, t, a.j, active);
-	if (!active) return;
+	static constexpr int R = 1 << LR;
+	static constexpr int CW = col_width(LR);
+	static constexpr int CWL = ilog2c(CW);
+	static constexpr int RS = CW + ((CW / 16 > 1) ? CW / 16 : 1);
+	static constexpr int PS = R * RS;                      // plane stride
+	static constexpr size_t SMEM = size_t(WMAX) * PS * 4;
+};
+
+template <int LC>
+struct RowShape
+{
+	static constexpr int C = 1 << LC;
+	static constexpr int PC = C + C / 32;
+	static constexpr size_t SMEM = size_t(WMAX) * PC * 4;
+};
+
+constexpr int FS_THREADS = 256;
+
+template <int SET, int LR>
+__device__ __forceinline__ void col_fwd_body(const Args &a, const TestDesc &d, uint32_t *sm)
+{
+	using S = ColShape<LR>;
+	constexpr int W = PrimeSet<SET>::W;
 	const int n = a.n, lc = n - LR;
 	const size_t N = size_t(1) << n, C = size_t(1) << lc;
-	const int c0 = blockIdx.x * CW;
+	const int c0 = blockIdx.x * S::CW;
 	const int32_t *src = d.regs + static_cast<size_t>(a.src) * N;
 	uint32_t *dst = (a.op == OP_FWD) ? d.zp : d.planes;
+	using MP = ColMap<S::RS>;
 
-	for (int e = threadIdx.x; e < R * CW; e += blockDim.x)
+	if (a.fix)
 	{
-		const int k = e >> CWL, cc = e & (CW - 1);
-		const int32_t dv = src[static_cast<size_t>(k) * C + c0 + cc];
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			sm[PL * R * RS + k * RS + cc] = ZS<SET, PL>::from_int(dv);
-		});
+		// pending carries: digits staged as int32 in the plane-0 area, one
+		// thread per 16-digit segment absorbs the incoming carry
+		int32_t *dg = reinterpret_cast<int32_t *>(sm);
+		for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
+		{
+			const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
+			const int4 v = *reinterpret_cast<const int4 *>(src + static_cast<size_t>(k) * C + c0 + cc);
+			int32_t *p = dg + MP::addr(k, cc);
+			p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
+		}
+		__syncthreads();
+		const size_t nseg = N / SEG;
+		int32_t *srcreg = d.regs + static_cast<size_t>(a.src) * N;
+		for (int e = threadIdx.x; e < S::R * (S::CW / SEG); e += blockDim.x)
+		{
+			const int k = e / (S::CW / SEG), sg = e % (S::CW / SEG);
+			const size_t j0 = static_cast<size_t>(k) * C + c0 + sg * SEG;
+			fix_segment(d, dg + MP::addr(k, sg * SEG), 1, srcreg + j0, carry_in(d, j0 / SEG, nseg), a.err);
+		}
+		__syncthreads();
+		for (int e = threadIdx.x; e < S::R * S::CW; e += blockDim.x)
+		{
+			const int k = e >> S::CWL, cc = e & (S::CW - 1);
+			const int i = MP::addr(k, cc);
+			const int32_t v = dg[i];
+			for_planes<SET>([&](auto PLc) {
+				constexpr int PL = decltype(PLc)::value;
+				if constexpr (PL > 0) sm[PL * S::PS + i] = ZS<SET, PL>::from_int(v);
+			});
+			sm[i] = ZS<SET, 0>::from_int(v);
+		}
+	}
+	else
+	{
+		for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
+		{
+			const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
+			const int4 v = *reinterpret_cast<const int4 *>(src + static_cast<size_t>(k) * C + c0 + cc);
+			for_planes<SET>([&](auto PLc) {
+				constexpr int PL = decltype(PLc)::value;
+				using Z = ZS<SET, PL>;
+				uint32_t *p = sm + PL * S::PS + MP::addr(k, cc);
+				p[0] = Z::from_int(v.x); p[1] = Z::from_int(v.y); p[2] = Z::from_int(v.z); p[3] = Z::from_int(v.w);
+			});
+		}
 	}
 	__syncthreads();
-	const ColMap mp{RS};
-	for_planes<SET>([&](auto PLc) {
-		constexpr int PL = decltype(PLc)::value;
-		run_fwd<SET, PL>(sm + PL * R * RS, mp, LR, CWL, true, 1u, 0u, a.tab.fw[PL], num_passes(LR));
-	});
-	for (int e = threadIdx.x; e < R * CW; e += blockDim.x)
+	run_fwd<SET, LR, false, MP>(sm, S::PS, S::CWL, true, 1u, 0u, a.tab[SET]);
+	for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
 	{
-		const int k = e >> CWL, cc = e & (CW - 1);
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			dst[PL * N + static_cast<size_t>(k) * C + c0 + cc] = sm[PL * R * RS + k * RS + cc];
-		});
+		const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
+#pragma unroll
+		for (int pl = 0; pl < W; ++pl)
+		{
+			const uint32_t *p = sm + pl * S::PS + MP::addr(k, cc);
+			*reinterpret_cast<uint4 *>(dst + pl * N + static_cast<size_t>(k) * C + c0 + cc) = make_uint4(p[0], p[1], p[2], p[3]);
+		}
 	}
 }
 
-// Rows: the last log2 C forward stages, pointwise, first inverse stages.
 template <int SET, int LC>
-__global__ void __launch_bounds__(256) k_row(const Args a)
+__device__ __forceinline__ void row_body(const Args &a, const TestDesc &d, uint32_t *sm)
 {
-	constexpr int C = 1 << LC;
-	constexpr int PC = C + C / 32;
-	extern __shared__ __align__(16) uint32_t sm[];
-	const int t = a.tests[blockIdx.y];
-	const TestDesc &d = a.desc[t];
-	bool active;
-	(void)get_dup(a, d, t, a.j, active);
-	if (!active) return;
+	using S = RowShape<LC>;
+	constexpr int W = PrimeSet<SET>::W;
 	const int n = a.n, lr = n - LC;
 	const size_t N = size_t(1) << n;
 	const int k = blockIdx.x;             // one row per CTA
-	uint32_t *buf = (a.op == OP_FWD) ? d.zp : d.planes;
-	const RowMap mp{LC};
+	uint32_t *buf = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(k) * S::C;
+	using MP = RowMap<LC>;
 
-	for_planes<SET>([&](auto PLc) {
-		constexpr int PL = decltype(PLc)::value;
-		const uint32_t *row = buf + PL * N + static_cast<size_t>(k) * C;
-		for (int i = threadIdx.x; i < C; i += blockDim.x) sm[PL * PC + mp(i, 0)] = row[i];
-	});
+#pragma unroll
+	for (int pl = 0; pl < W; ++pl)
+		for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
+		{
+			const uint4 u = *reinterpret_cast<const uint4 *>(buf + pl * N + 4 * e);
+			uint32_t *p = sm + pl * S::PC + MP::addr(4 * e, 0);
+			p[0] = u.x; p[1] = u.y; p[2] = u.z; p[3] = u.w;
+		}
 	__syncthreads();
-	for_planes<SET>([&](auto PLc) {
-		constexpr int PL = decltype(PLc)::value;
-		row_core<SET, PL>(sm + PL * PC, mp, LC, 0, (1u << lr) + static_cast<uint32_t>(k), a.tab.fw[PL], a.tab.iv[PL],
-						  d.zp + PL * N + static_cast<size_t>(k) * C, a.op);
-	});
-	for_planes<SET>([&](auto PLc) {
-		constexpr int PL = decltype(PLc)::value;
-		uint32_t *row = buf + PL * N + static_cast<size_t>(k) * C;
-		for (int i = threadIdx.x; i < C; i += blockDim.x) row[i] = sm[PL * PC + mp(i, 0)];
-	});
+	row_core<SET, LC, MP>(sm, S::PC, 0, (1u << lr) + static_cast<uint32_t>(k), a.tab[SET],
+						  d.zp + static_cast<size_t>(k) * S::C, N, a.op);
+#pragma unroll
+	for (int pl = 0; pl < W; ++pl)
+		for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
+		{
+			const uint32_t *p = sm + pl * S::PC + MP::addr(4 * e, 0);
+			*reinterpret_cast<uint4 *>(buf + pl * N + 4 * e) = make_uint4(p[0], p[1], p[2], p[3]);
+		}
 }
 
-// Columns: last log2 R inverse stages, CRT, carry inside 16-digit segments.
 template <int SET, int LR>
-__global__ void __launch_bounds__(256) k_col_inv(const Args a)
+__device__ __forceinline__ void col_inv_body(const Args &a, const TestDesc &d, bool dup, uint32_t *sm)
 {
-	constexpr int R = 1 << LR, CW = col_width(LR), RS = col_stride(LR);
-	constexpr int CWL = (CW == 16) ? 4 : ((CW == 32) ? 5 : ((CW == 64) ? 6 : ((CW == 128) ? 7 : ((CW == 256) ? 8 : 9))));
-	constexpr int SPR = CW / SEG;        // segments per tile row
-	extern __shared__ __align__(16) uint32_t sm[];
-	const int t = a.tests[blockIdx.y];
-	const TestDesc &d = a.desc[t];
-	bool active;
-	const bool dup = get_dup(a, d, t, a.j, active);
-	if (!active) return;
+	using S = ColShape<LR>;
+	constexpr int W = PrimeSet<SET>::W;
+	constexpr int SPR = S::CW / SEG;      // segments per tile row
 	const int n = a.n, lc = n - LR;
 	const size_t N = size_t(1) << n, C = size_t(1) << lc;
-	const int c0 = blockIdx.x * CW;
-	const uint32_t b = d.b;
-	const uint64_t binv = d.binv;
+	const int c0 = blockIdx.x * S::CW;
+	using MP = ColMap<S::RS>;
 
-	for (int e = threadIdx.x; e < R * CW; e += blockDim.x)
+	for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
 	{
-		const int k = e >> CWL, cc = e & (CW - 1);
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			sm[PL * R * RS + k * RS + cc] = d.planes[PL * N + static_cast<size_t>(k) * C + c0 + cc];
-		});
+		const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
+#pragma unroll
+		for (int pl = 0; pl < W; ++pl)
+		{
+			const uint4 u = *reinterpret_cast<const uint4 *>(d.planes + pl * N + static_cast<size_t>(k) * C + c0 + cc);
+			uint32_t *p = sm + pl * S::PS + MP::addr(k, cc);
+			p[0] = u.x; p[1] = u.y; p[2] = u.z; p[3] = u.w;
+		}
 	}
 	__syncthreads();
-	const ColMap mp{RS};
-	for_planes<SET>([&](auto PLc) {
-		constexpr int PL = decltype(PLc)::value;
-		run_inv<SET, PL>(sm + PL * R * RS, mp, LR, CWL, true, 1u, 0u, a.tab.fw[PL], a.tab.iv[PL], num_passes(LR));
-	});
+	run_inv<SET, LR, false, MP>(sm, S::PS, S::CWL, true, 1u, 0u, a.tab[SET]);
 
 	int32_t *out = d.regs + static_cast<size_t>(a.dst) * N;
-	for (int e = threadIdx.x; e < R * SPR; e += blockDim.x)
+	for (int e = threadIdx.x; e < S::R * SPR; e += blockDim.x)
 	{
 		const int k = e / SPR, s = e % SPR;
 		const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
@@ -510,19 +536,179 @@ __global__ void __launch_bounds__(256) k_col_inv(const Args a)
 		for (int i = 0; i < SEG; ++i)
 		{
 			uint32_t x[3];
-			for_planes<SET>([&](auto PLc) {
-				constexpr int PL = decltype(PLc)::value;
-				x[PL] = sm[PL * R * RS + k * RS + s * SEG + i];
-			});
-			i128 v = crt<SET>(x);
-			if (dup) v += v;
-			dg[i] = digit_carry(v + c, b, binv, c);
+#pragma unroll
+			for (int pl = 0; pl < W; ++pl) x[pl] = sm[pl * S::PS + MP::addr(k, s * SEG + i)];
+			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
 		}
 		int4 *o = reinterpret_cast<int4 *>(out + j0);
 #pragma unroll
 		for (int i = 0; i < SEG / 4; ++i) o[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
 		d.carry[j0 / SEG] = c;
 	}
+}
+
+// Columns: tile of CW columns x R rows; first log2 R forward stages.
+template <int LR>
+__global__ void __launch_bounds__(FS_THREADS) k_col_fwd(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) col_fwd_body<0, LR>(a, d, sm); else col_fwd_body<1, LR>(a, d, sm);
+}
+
+// Rows: the last log2 C forward stages, pointwise, first inverse stages.
+template <int LC>
+__global__ void __launch_bounds__(FS_THREADS) k_row(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) row_body<0, LC>(a, d, sm); else row_body<1, LC>(a, d, sm);
+}
+
+// Columns: last log2 R inverse stages, CRT, carry inside 16-digit segments.
+template <int LR>
+__global__ void __launch_bounds__(FS_THREADS) k_col_inv(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	const bool dup = get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) col_inv_body<0, LR>(a, d, dup, sm); else col_inv_body<1, LR>(a, d, dup, sm);
+}
+
+// ---- four-step with R <= 16 rows: one thread owns a whole column.
+
+constexpr int COLR_THREADS = 256;
+
+template <int SET, int LR>
+__device__ __forceinline__ void col_fwd_reg_body(const Args &a, const TestDesc &d, int32_t *sm)
+{
+	constexpr int R = 1 << LR, T = COLR_THREADS;
+	const int n = a.n;
+	const size_t N = size_t(1) << n, C = size_t(1) << (n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x;
+	int32_t *const srcreg = d.regs + static_cast<size_t>(a.src) * N;
+	const int32_t *src = srcreg + c0 + tid;
+	uint32_t *dst = ((a.op == OP_FWD) ? d.zp : d.planes) + c0 + tid;
+	int32_t dv[R];
+#pragma unroll
+	for (int k = 0; k < R; ++k) dv[k] = src[k * C];
+	if (a.fix)
+	{
+		// pending carries: stage the tile [R][T], one thread per 16-digit segment
+#pragma unroll
+		for (int k = 0; k < R; ++k) sm[k * (T + 1) + tid] = dv[k];
+		__syncthreads();
+		const size_t nseg = N / SEG;
+		for (int e = tid; e < R * (T / SEG); e += T)
+		{
+			const int k = e / (T / SEG), s = e % (T / SEG);
+			const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
+			fix_segment(d, sm + k * (T + 1) + s * SEG, 1, srcreg + j0, carry_in(d, j0 / SEG, nseg), a.err);
+		}
+		__syncthreads();
+#pragma unroll
+		for (int k = 0; k < R; ++k) dv[k] = sm[k * (T + 1) + tid];
+	}
+	for_planes<SET>([&](auto PLc) {
+		constexpr int PL = decltype(PLc)::value;
+		using Z = ZS<SET, PL>;
+		uint32_t x[R];
+#pragma unroll
+		for (int k = 0; k < R; ++k) x[k] = Z::from_int(dv[k]);
+		fwd_reg<Z, LR>(Z{}, x, 1u, a.tab[SET].fw[PL]);
+#pragma unroll
+		for (int k = 0; k < R; ++k) dst[PL * N + k * C] = x[k];
+	});
+}
+
+// Inverse column transform in registers, then the tile (R rows x 256
+// columns) goes through shared memory so that each thread takes one 16-digit
+// row segment for CRT and carry.
+template <int SET, int LR>
+__device__ __forceinline__ void col_inv_reg_body(const Args &a, const TestDesc &d, bool dup, uint32_t *sm)
+{
+	constexpr int R = 1 << LR, W = PrimeSet<SET>::W;
+	constexpr int T = COLR_THREADS, RS = T + T / 16, PS = R * RS, SPR = T / SEG;
+	const int n = a.n;
+	const size_t N = size_t(1) << n, C = size_t(1) << (n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x;
+	using MP = ColMap<RS>;
+	for_planes<SET>([&](auto PLc) {
+		constexpr int PL = decltype(PLc)::value;
+		using Z = ZS<SET, PL>;
+		const uint32_t *src = d.planes + PL * N + c0 + tid;
+		uint32_t x[R];
+#pragma unroll
+		for (int k = 0; k < R; ++k) x[k] = src[k * C];
+		inv_reg<Z, LR>(Z{}, x, 1u, a.tab[SET].iv[PL], true, __ldg(&a.tab[SET].fw[PL][0]), __ldg(&a.tab[SET].iv[PL][0]));
+#pragma unroll
+		for (int k = 0; k < R; ++k) sm[PL * PS + MP::addr(k, tid)] = x[k];
+	});
+	__syncthreads();
+	int32_t *out = d.regs + static_cast<size_t>(a.dst) * N;
+	for (int e = tid; e < R * SPR; e += T)
+	{
+		const int k = e / SPR, s = e % SPR;
+		const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
+		int64_t cr = 0;
+		int32_t dg[SEG];
+#pragma unroll
+		for (int i = 0; i < SEG; ++i)
+		{
+			uint32_t x[3];
+#pragma unroll
+			for (int pl = 0; pl < W; ++pl) x[pl] = sm[pl * PS + MP::addr(k, s * SEG + i)];
+			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, cr);
+		}
+		int4 *o = reinterpret_cast<int4 *>(out + j0);
+#pragma unroll
+		for (int i = 0; i < SEG / 4; ++i) o[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
+		d.carry[j0 / SEG] = cr;
+	}
+}
+
+// Shared memory: [R][T + 1] int32 staging of the digits when fixing carries.
+template <int LR>
+__global__ void __launch_bounds__(COLR_THREADS) k_colr_fwd(const Args a)
+{
+	__shared__ int32_t sm[(1 << LR) * (COLR_THREADS + 1)];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) col_fwd_reg_body<0, LR>(a, d, sm); else col_fwd_reg_body<1, LR>(a, d, sm);
+}
+
+template <int LR>
+struct ColRegShape
+{
+	static constexpr size_t SMEM = size_t(WMAX) * (1 << LR) * (COLR_THREADS + COLR_THREADS / 16) * 4;
+};
+
+template <int LR>
+__global__ void __launch_bounds__(COLR_THREADS) k_colr_inv(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	const bool dup = get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) col_inv_reg_body<0, LR>(a, d, dup, sm); else col_inv_reg_body<1, LR>(a, d, dup, sm);
 }
 
 // Each segment absorbs the carry of the previous one (segment 0 takes minus
@@ -548,7 +734,7 @@ __global__ void __launch_bounds__(256) k_fixup(const Args a)
 		const int4 v = p[i];
 		dg[4 * i] = v.x; dg[4 * i + 1] = v.y; dg[4 * i + 2] = v.z; dg[4 * i + 3] = v.w;
 	}
-	if (!absorb<SEG>(dg, cin, d.b, d.binv)) atomicOr(a.err, 1u);
+	if (!absorb<SEG>(dg, cin, d.ck)) atomicOr(a.err, 1u);
 #pragma unroll
 	for (int i = 0; i < SEG / 4; ++i) p[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
 }

@@ -21,49 +21,60 @@
 
 namespace gfc {
 
+// Z: arithmetic of one prime (Zp with the prime as a constant, or ZpR with
+// the prime in registers).
 template <class Z>
-__device__ __forceinline__ void bfly_ct(uint32_t &a, uint32_t &b, uint32_t w)
+__device__ __forceinline__ void bfly_ct(const Z &z, uint32_t &a, uint32_t &b, uint32_t w)
 {
-	const uint32_t t = Z::mul(b, w);
-	b = Z::sub(a, t);
-	a = Z::add(a, t);
+	const uint32_t t = z.mul(b, w);
+	b = z.sub(a, t);
+	a = z.add(a, t);
 }
 
 template <class Z>
-__device__ __forceinline__ void bfly_gs(uint32_t &a, uint32_t &b, uint32_t wi)
+__device__ __forceinline__ void bfly_gs(const Z &z, uint32_t &a, uint32_t &b, uint32_t wi)
 {
-	const uint32_t t = Z::sub(a, b);
-	a = Z::add(a, b);
-	b = Z::mul(t, wi);
+	const uint32_t t = z.sub(a, b);
+	a = z.add(a, b);
+	b = z.mul(t, wi);
 }
 
 // r forward stages on 2^r registers.  Stage t of the group uses the table
 // entries (tbase << t) + sb, sb < 2^t, with tbase = (base << sigma) + blk.
+// All 2^r - 1 roots are loaded before the first butterfly.
 template <class Z, int r>
-__device__ __forceinline__ void fwd_reg(uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ tw)
+__device__ __forceinline__ void fwd_reg(const Z &z, uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ tw)
 {
+	uint32_t w[(1 << r) - 1];
+#pragma unroll
+	for (int t = 0; t < r; ++t)
+#pragma unroll
+		for (int sb = 0; sb < (1 << t); ++sb) w[(1 << t) - 1 + sb] = __ldg(&tw[(tbase << t) + sb]);
 #pragma unroll
 	for (int t = 0; t < r; ++t)
 	{
 		const int half = 1 << (r - 1 - t);
 #pragma unroll
 		for (int sb = 0; sb < (1 << t); ++sb)
-		{
-			const uint32_t w = __ldg(&tw[(tbase << t) + sb]);
 #pragma unroll
-			for (int m = 0; m < half; ++m) bfly_ct<Z>(x[sb * 2 * half + m], x[sb * 2 * half + m + half], w);
-		}
+			for (int m = 0; m < half; ++m)
+				bfly_ct(z, x[sb * 2 * half + m], x[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
 	}
 }
 
 // r inverse stages (reverse order).  When `norm` is set the group contains
 // global stage 0 (tbase == 1): its butterflies also multiply both outputs by
-// the normalisation, a' = (a + b) c, b' = (a - b) K, with c = twi_fwd0 and
-// K = twi[0] prepared on the host.
+// the normalisation, a' = (a + b) c, b' = (a - b) K, with c = fw[0] and
+// K = iv[0] prepared on the host.
 template <class Z, int r>
-__device__ __forceinline__ void inv_reg(uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ twi,
+__device__ __forceinline__ void inv_reg(const Z &z, uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ twi,
 										bool norm, uint32_t c_norm, uint32_t k_norm)
 {
+	uint32_t w[(1 << r) - 1];
+#pragma unroll
+	for (int t = 0; t < r; ++t)
+#pragma unroll
+		for (int sb = 0; sb < (1 << t); ++sb) w[(1 << t) - 1 + sb] = __ldg(&twi[(tbase << t) + sb]);
 #pragma unroll
 	for (int t = r - 1; t >= 0; --t)
 	{
@@ -77,37 +88,46 @@ __device__ __forceinline__ void inv_reg(uint32_t (&x)[1 << r], uint32_t tbase, c
 				for (int m = 0; m < half; ++m)
 				{
 					uint32_t &a = x[m], &b = x[m + half];
-					const uint32_t d = Z::sub(a, b);
-					a = Z::mul(Z::add(a, b), c_norm);
-					b = Z::mul(d, k_norm);
+					const uint32_t d = z.sub(a, b);
+					a = z.mul(z.add(a, b), c_norm);
+					b = z.mul(d, k_norm);
 				}
 			}
 			else
 			{
-				const uint32_t wi = __ldg(&twi[(tbase << t) + sb]);
 #pragma unroll
-				for (int m = 0; m < half; ++m) bfly_gs<Z>(x[sb * 2 * half + m], x[sb * 2 * half + m + half], wi);
+				for (int m = 0; m < half; ++m)
+					bfly_gs(z, x[sb * 2 * half + m], x[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
 			}
 		}
 	}
 }
 
-// Shared-memory address maps.
-// Rows: `lanes` contiguous transforms of length 2^l, padded one word per 32.
+// Shared-memory address maps.  addr(i, lane) places element i of transform
+// `lane`; off(m, step) is the address offset of element i0 + m step from
+// element i0 for the groups the passes form (where it is independent of i0).
+// Rows: transforms of length 2^L stored back to back, one padding word per 32.
+// In a pass group either step >= 32, or i0 mod 32 + m step stays below 32,
+// so the padding term is linear in m.
+template <int L>
 struct RowMap
 {
-	int l;
-	__device__ __forceinline__ int operator()(int i, int lane) const
+	__device__ __forceinline__ static int addr(int i, int lane)
 	{
-		const int a = (lane << l) + i;
+		const int a = (lane << L) + i;
 		return a + (a >> 5);
 	}
+	__host__ __device__ static constexpr int off(int m, int step) { return m * step + ((m * step) >> 5); }
 };
-// Columns: tile [2^l][RS] with the transform index i on the slow axis.
+// Columns: tile [2^l][RS] with the transform index i on the slow axis and
+// one padding word after every 16 columns, so that both a warp reading 32
+// consecutive columns and a warp reading one 16-digit segment per thread are
+// free of bank conflicts.
+template <int RS>
 struct ColMap
 {
-	int RS;
-	__device__ __forceinline__ int operator()(int i, int lane) const { return i * RS + lane; }
+	__device__ __forceinline__ static int addr(int i, int lane) { return i * RS + lane + (lane >> 4); }
+	__host__ __device__ static constexpr int off(int m, int step) { return m * step * RS; }
 };
 
 // Group geometry of a radix-2^r pass at local stage sigma of a length-2^l

@@ -56,7 +56,7 @@ def test_single_cta_plan(oracle, n, b):
     check_ops(oracle, b, n, seed=n)
 
 
-@pytest.mark.parametrize("n,lr", [(14, 3), (12, 4), (13, 5), (14, 6), (12, 3), (15, 3), (15, 7), (16, 4), (16, 8),
+@pytest.mark.parametrize("n,lr", [(11, 3), (14, 3), (12, 4), (13, 5), (14, 6), (12, 3), (15, 3), (15, 7), (16, 4), (16, 8),
                                   (17, 9), (18, 10)])
 @pytest.mark.parametrize("b", [SMALL_B, LARGE_B])
 def test_four_step_plan(oracle, n, lr, b):
