@@ -71,6 +71,8 @@ SIGNATURES = {
     "gfc_graph_destroy": (None, [vp]),
     "gfc_launch_count": (ctypes.c_uint64, []),
     "gfc_probe_int_throughput": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "gfc_square_noalloc": (ctypes.c_int, [c_i32p, c_i32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                          ctypes.c_uint32, ctypes.c_int, vp]),
     "gfc_gint_unbalance": (None, [c_i32p, ctypes.c_size_t, ctypes.c_uint32]),
     "gfc_gint_balance": (None, [c_i32p, ctypes.c_size_t, ctypes.c_uint32]),
     "gfc_gint_is_one": (ctypes.c_int, [c_i32p, ctypes.c_size_t, ctypes.c_uint32, c_u64p, c_u64p]),

@@ -1054,3 +1054,180 @@ GFC_API int gfc_graph_launch(gfc_graph *g)
 }
 
 GFC_API void gfc_graph_destroy(gfc_graph *g) { delete g; }
+
+// ------------------------------------------------------------------ squaring without allocation
+//
+// gfc_square_noalloc runs the four-step squaring with all of its scratch
+// (root tables, transform planes, segment carries, test descriptor) in one
+// file-scope device array instead of memory from cudaMalloc.  It exists for
+// callers that cannot allocate device memory when they square: code running
+// inside another runtime's memory pool or allocator lock, processes whose
+// device-memory budget is fixed at start-up, and hosts that forbid
+// allocation after initialisation.  The array is part of the library image,
+// so every GPU that loads the library holds it until the process exits.
+
+namespace {
+
+constexpr int NA_MIN_LOGN = 12, NA_MAX_LOGN = 16, NA_LR = 4;
+constexpr size_t NA_N = size_t(1) << NA_MAX_LOGN;
+// Layout in 32-bit words.
+constexpr size_t NA_OFF_TAB = 0;                                  // 5 primes x (forward, inverse) x N
+constexpr size_t NA_OFF_PLANES = NA_OFF_TAB + 10 * NA_N;          // 3 planes x N
+constexpr size_t NA_OFF_CARRY = NA_OFF_PLANES + 3 * NA_N;         // N/16 int64 carries
+constexpr size_t NA_OFF_DESC = NA_OFF_CARRY + NA_N / 8;           // one TestDesc
+constexpr size_t NA_OFF_MISC = NA_OFF_DESC + 64;                  // test index, position, error word
+constexpr size_t NA_WORDS = NA_OFF_MISC + 64;                     // 3.44 MB
+static_assert(sizeof(TestDesc) <= 64 * sizeof(uint32_t), "descriptor slot");
+
+static __device__ __align__(256) uint32_t g_na_scratch[NA_WORDS];
+
+constexpr int NA_MAX_DEVICES = 64;
+struct NaDevice
+{
+	uint32_t *base = nullptr;   // device address of g_na_scratch on this device
+	int tab_n = 0;              // n of the root tables currently stored
+};
+std::mutex g_na_mu;
+NaDevice g_na_dev[NA_MAX_DEVICES];
+uint32_t g_na_pw[NA_N + 1], g_na_fw[NA_N], g_na_iv[NA_N];   // host staging for the root tables
+
+// Smallest generator of (Z/pZ)* without heap use (p - 1 has < 10 prime factors).
+uint32_t na_primitive_root(uint32_t p)
+{
+	uint32_t f[16];
+	int nf = 0;
+	uint32_t m = p - 1;
+	for (uint32_t q = 2; static_cast<uint64_t>(q) * q <= m; ++q)
+		if (m % q == 0) { f[nf++] = q; while (m % q == 0) m /= q; }
+	if (m > 1) f[nf++] = m;
+	for (uint32_t g = 2;; ++g)
+	{
+		bool ok = true;
+		for (int i = 0; i < nf; ++i) if (powmod_h(g, (p - 1) / f[i], p) == 1) { ok = false; break; }
+		if (ok) return g;
+	}
+}
+
+// The root tables of build_roots(), written into the host staging arrays.
+void na_build_roots(uint32_t p, int n)
+{
+	const uint32_t N = 1u << n;
+	const uint32_t psi = powmod_h(na_primitive_root(p), (p - 1) / (2ull * N), p);
+	g_na_pw[0] = 1;
+	for (uint32_t i = 1; i <= N; ++i) g_na_pw[i] = mulmod_h(g_na_pw[i - 1], psi, p);
+	for (uint32_t k = 1; k < N; ++k)
+	{
+		const uint32_t e = bitrev(k, n);
+		g_na_fw[k] = to_mont_h(g_na_pw[e], p);
+		g_na_iv[k] = to_mont_h(p - g_na_pw[N - e], p);
+	}
+	const uint32_t R1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
+	const uint32_t c = mulmod_h(mulmod_h(R1, R1, p), powmod_h(N % p, p - 2, p), p);
+	g_na_fw[0] = c;
+	g_na_iv[0] = mulmod_h(p - g_na_pw[N / 2], c, p);
+}
+
+// Per-device set-up (first call on a device): the device address of the
+// scratch array, and the root tables for n whenever n changes.
+NaDevice &na_setup(int device, int n)
+{
+	if ((device < 0) || (device >= NA_MAX_DEVICES)) fail(GFC_ERR_ARG, "square_noalloc: device ordinal out of range");
+	NaDevice &nd = g_na_dev[device];
+	if (nd.base == nullptr)
+	{
+		void *p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
+		if (e != cudaSuccess) fail(GFC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+		nd.base = static_cast<uint32_t *>(p);
+	}
+	if (nd.tab_n != n)
+	{
+		const size_t N = size_t(1) << n;
+		nd.tab_n = 0;
+		for (int s = 0; s < 5; ++s)
+		{
+			na_build_roots(kPrime[s], n);
+			GFC_CK(cudaMemcpy(nd.base + NA_OFF_TAB + (2 * s) * NA_N, g_na_fw, N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+			GFC_CK(cudaMemcpy(nd.base + NA_OFF_TAB + (2 * s + 1) * NA_N, g_na_iv, N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		}
+		nd.tab_n = n;
+	}
+	return nd;
+}
+
+}  // namespace
+
+GFC_API int gfc_square_noalloc(const int32_t *in, int32_t *out, uint32_t b, uint32_t n, int dup, uint32_t count,
+							   int device, void *stream)
+{
+	return guard([&] {
+		if ((in == nullptr) || (out == nullptr)) fail(GFC_ERR_ARG, "square_noalloc: null digit pointer");
+		if ((n < NA_MIN_LOGN) || (n > NA_MAX_LOGN))
+			fail(GFC_ERR_ARG, "square_noalloc: n must satisfy 12 <= n <= 16 (size of the static scratch array)");
+		if ((b < 8) || (b >= (1u << 31))) fail(GFC_ERR_ARG, "square_noalloc: base b must satisfy 8 <= b < 2^31");
+		const int set = choose_set(b, static_cast<int>(n));
+		if (set < 0) fail(GFC_ERR_RANGE, "square_noalloc: (b, n) is outside the exact range of the RNS prime sets");
+		std::lock_guard<std::mutex> lock(g_na_mu);
+		GFC_CK(cudaSetDevice(device));
+		NaDevice &nd = na_setup(device, static_cast<int>(n));
+		const cudaStream_t s = static_cast<cudaStream_t>(stream);
+		const size_t N = size_t(1) << n;
+		uint32_t *const base = nd.base;
+
+		// descriptor of the single test, read by the kernels from the scratch array
+		TestDesc d{};
+		d.regs = out;
+		d.planes = base + NA_OFF_PLANES;
+		d.zp = base + NA_OFF_PLANES;
+		d.carry = reinterpret_cast<int64_t *>(base + NA_OFF_CARRY);
+		d.ebits = nullptr;
+		d.ck = carry_constants(b, set);
+		d.b = b;
+		d.set = set;
+		struct { int32_t test; int32_t pad; int64_t pos; uint32_t err; } misc = { 0, 0, 0, 0 };
+		GFC_CK(cudaMemcpyAsync(base + NA_OFF_DESC, &d, sizeof(d), cudaMemcpyHostToDevice, s));
+		// the error word must start at zero; planes and carries are written before they are read
+		GFC_CK(cudaMemcpyAsync(base + NA_OFF_MISC, &misc, sizeof(misc), cudaMemcpyHostToDevice, s));
+		if (in != out) GFC_CK(cudaMemcpyAsync(out, in, N * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+
+		Args a{};
+		a.desc = reinterpret_cast<const TestDesc *>(base + NA_OFF_DESC);
+		a.tests = reinterpret_cast<const int32_t *>(base + NA_OFF_MISC);
+		a.pos = reinterpret_cast<int64_t *>(base + NA_OFF_MISC + 2);
+		a.err = base + NA_OFF_MISC + 4;
+		const int slot0[2] = { 0, 2 };
+		for (int st = 0; st < 2; ++st)
+			for (int pl = 0; pl < 3; ++pl)
+			{
+				const int k = (st == 0 && pl == 2) ? 1 : slot0[st] + pl;
+				a.tab[st].fw[pl] = base + NA_OFF_TAB + (2 * k) * NA_N;
+				a.tab[st].iv[pl] = base + NA_OFF_TAB + (2 * k + 1) * NA_N;
+			}
+		a.n = static_cast<int>(n);
+		a.lr = NA_LR;
+		a.num_regs = 1;
+		a.op = OP_SQUARE;
+		a.dup_mode = dup ? DUP_ALL : DUP_NONE;
+
+		const int lc = static_cast<int>(n) - NA_LR;
+		launch_col(NA_LR, false, a, 0, nullptr, true);
+		launch_row(lc, a, 0, nullptr, true);
+		for (uint32_t j = 0; j < count; ++j)
+		{
+			a.fix = (j > 0) ? 1 : 0;   // carries of the previous squaring are absorbed on load
+			launch_col(NA_LR, false, a, 1, s, false);
+			launch_row(lc, a, 1, s, false);
+			launch_col(NA_LR, true, a, 1, s, false);
+		}
+		if (count > 0)
+		{
+			const dim3 grid(static_cast<unsigned>((N / SEG + 255) / 256), 1u);
+			k_fixup<<<grid, 256, 0, s>>>(a);
+			after_launch();
+		}
+		uint32_t err = 0;
+		GFC_CK(cudaMemcpyAsync(&err, base + NA_OFF_MISC + 4, sizeof(err), cudaMemcpyDeviceToHost, s));
+		GFC_CK(cudaStreamSynchronize(s));
+		if (err != 0) fail(GFC_ERR_NUMERIC, "square_noalloc: a segment carry was not absorbed");
+	});
+}

@@ -190,6 +190,29 @@ int gfc_batch_time_kernels(gfc_batch *bt, uint32_t reps, float *ms);
  * butterfly 31-bit.  The roofline denominator for the squaring kernels. */
 int gfc_probe_int_throughput(int device, double *out);
 
+/* ------------------------------------------------------------------ squaring without allocation
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory at the point they square (code inside another runtime's memory pool
+ * or allocator lock, processes with a device-memory budget fixed at start-up,
+ * hosts that forbid allocation after initialisation): count squarings (dup
+ * as in gfc_square_dup) of the N = 2^n digits at device address `in`, result
+ * at device address `out` (may equal `in`), on `stream` (NULL: the default
+ * stream) of `device`.  The input digits must satisfy |d| <= b/2 + 1.
+ *  - All scratch (root tables, transform planes, carries) lives in one
+ *    static device array of 3.44 MB that every GPU loading the library holds
+ *    until the process exits; the call makes no cudaMalloc/cudaFree and no
+ *    allocating library call.  Hence 12 <= n <= 16; larger n returns
+ *    GFC_ERR_ARG.
+ *  - The first call on a device resolves the array's device address and
+ *    builds its root tables (again whenever n changes); make that first call
+ *    before any stream capture.
+ *  - Every call shares the array: calls that overlap on the GPU (other
+ *    streams, other host threads without ordering) race.  The call waits for
+ *    `stream` before returning and reports a device-side carry failure as
+ *    GFC_ERR_NUMERIC. */
+int gfc_square_noalloc(const int32_t *in, int32_t *out, uint32_t b, uint32_t n, int dup, uint32_t count, int device,
+					   void *stream);
+
 /* ------------------------------------------------------------------ residues (host)
  * genefer's gint utilities on N host digits (src/gint.h:40-225). */
 

@@ -1,0 +1,58 @@
+"""gfc_square_noalloc: the squaring entry point for callers that cannot
+allocate device memory when they square (it keeps its scratch in a static
+device array).  Its output must equal the regular engine's, on two calls in a
+row.  This file is collected last so that a failure here leaves every other
+test already run."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from genefer22_b200 import Transform, gint
+from genefer22_b200._lib import GFC_OK, c_i32p, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _ptr(t):
+    return ctypes.cast(ctypes.c_void_p(t.data_ptr()), c_i32p)
+
+
+@pytest.mark.parametrize("b,n", [(50_000_002, 16), (1_000_002, 12), (1_999_999_998, 14)])
+def test_square_noalloc_matches_engine(b, n):
+    import torch
+    rng = np.random.default_rng(n)
+    x = gint.balance(rng.integers(-(b // 2), b // 2 + 1, size=1 << n).astype(np.int32), b)
+    t = Transform(b, n)
+    t.setInt(x)
+    cur = torch.tensor(x, dtype=torch.int32, device="cuda:0")
+    out = torch.empty_like(cur)
+    torch.cuda.synchronize()
+    for call, (dup, count) in enumerate(((1, 3), (0, 2))):
+        rc = lib().gfc_square_noalloc(_ptr(cur), _ptr(out), b, n, dup, count, 0, None)
+        assert rc == GFC_OK, lib().gfc_last_error().decode()
+        for _ in range(count):
+            t.squareDup(bool(dup))
+        got = out.cpu().numpy()
+        assert np.abs(got).max() <= b // 2 + 1
+        assert np.array_equal(gint.unbalance(got, b), gint.unbalance(t.getInt(), b)), f"call {call}"
+        cur, out = out, cur
+
+
+def test_square_noalloc_in_place_and_limits():
+    import torch
+    b, n = 1_000_002, 13
+    rng = np.random.default_rng(5)
+    x = gint.balance(rng.integers(-(b // 2), b // 2 + 1, size=1 << n).astype(np.int32), b)
+    t = Transform(b, n)
+    t.setInt(x)
+    buf = torch.tensor(x, dtype=torch.int32, device="cuda:0")
+    torch.cuda.synchronize()
+    for _ in range(2):
+        assert lib().gfc_square_noalloc(_ptr(buf), _ptr(buf), b, n, 0, 1, 0, None) == GFC_OK
+        t.squareDup(False)
+        assert np.array_equal(gint.unbalance(buf.cpu().numpy(), b), gint.unbalance(t.getInt(), b))
+    big = torch.zeros(1 << 17, dtype=torch.int32, device="cuda:0")
+    torch.cuda.synchronize()
+    assert lib().gfc_square_noalloc(_ptr(big), _ptr(big), b, 17, 0, 1, 0, None) == -1
+    assert b"12 <= n <= 16" in lib().gfc_last_error()
