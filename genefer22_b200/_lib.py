@@ -29,6 +29,7 @@ SIGNATURES = {
     "gfc_destroy": (None, [vp]),
     "gfc_set": (ctypes.c_int, [vp, ctypes.c_uint32]),
     "gfc_square_dup": (ctypes.c_int, [vp, ctypes.c_int]),
+    "gfc_square_mul": (ctypes.c_int, [vp, ctypes.c_int32]),
     "gfc_init_multiplicand": (ctypes.c_int, [vp, ctypes.c_size_t]),
     "gfc_mul": (ctypes.c_int, [vp]),
     "gfc_copy": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_size_t]),

@@ -192,10 +192,11 @@ __device__ __forceinline__ uint64_t divb64(uint64_t n, uint32_t b, uint64_t binv
 // set (p1 for set 0, p1 p2 for set 1) and M the product of its primes:
 //   q[f-1] = floor(f T / b), r[f-1] = f T mod b,
 //   mq[f-1] = floor(f M / b) mod 2^64, mr[f-1] = f M mod b,
-//   K = ceil(2^56 / b), kb = K b.
+//   K = ceil(2^56 / b), kb = K b;  K' = ceil(2^62 / b), kwb = K' b.
 struct CarryK
 {
 	uint64_t binv, kb, k;
+	uint64_t kw, kwb;       // K' = ceil(2^62 / b), K' b: the same for |s| < 2^62
 	uint64_t q[2], mq[2];
 	uint32_t r[2], mr[2];
 	uint32_t b, h;
@@ -244,6 +245,15 @@ __device__ __forceinline__ int32_t crt_carry<1>(const uint32_t x[3], int dup, co
 	uint64_t rv;
 	const uint64_t qv = divb64(U + static_cast<uint64_t>(c) + K.kb, K.b, K.binv, rv);
 	c = static_cast<int64_t>(qv + K.q[dup] * a3 - (z ? K.mq[dup] + 1 : 0) - K.k);
+	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
+}
+
+// Balanced digit of s (|s| < 2^62) and carry floor((s + b/2) / b).
+__device__ __forceinline__ int32_t carry_wide(int64_t s, const CarryK &K, int64_t &c)
+{
+	uint64_t rv;
+	const uint64_t qv = divb64(static_cast<uint64_t>(s) + K.h + K.kwb, K.b, K.binv, rv);
+	c = static_cast<int64_t>(qv - K.kw);
 	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
 }
 

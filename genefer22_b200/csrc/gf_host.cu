@@ -181,6 +181,8 @@ CarryK carry_constants(uint32_t b, int set)
 	k.binv = ~uint64_t(0) / b;
 	k.k = ((uint64_t(1) << 56) + b - 1) / b;
 	k.kb = k.k * b;
+	k.kw = ((uint64_t(1) << 62) + b - 1) / b;
+	k.kwb = k.kw * b;
 	for (int f = 1; f <= 2; ++f)
 	{
 		k.q[f - 1] = static_cast<uint64_t>((f * T) / b);
@@ -476,6 +478,22 @@ void op_square(gfc_batch &bt, int dup_mode, uint32_t count)
 	}
 }
 
+// r_0 = a r_0^2 for all tests (transform::squareMul, src/transform.h:60).
+void op_square_mul(gfc_batch &bt, int32_t m)
+{
+	if (m == 1 || m == 2) { op_square(bt, (m == 2) ? DUP_ALL : DUP_NONE, 1); return; }
+	op_square(bt, DUP_NONE, 1);
+	materialize(bt);
+	Args a = make_args(bt);
+	a.dup_mode = DUP_NONE;
+	a.dst = 0;
+	const unsigned nseg = static_cast<unsigned>(bt.N / SEG);
+	const dim3 grid((nseg + FIX_THREADS - 1) / FIX_THREADS, static_cast<unsigned>(bt.count));
+	k_mulscalar<<<grid, FIX_THREADS, 0, bt.stream>>>(a, m);
+	after_launch();
+	bt.pending = 0;
+}
+
 // r_m = transform(r_src) for all tests.
 void op_init_multiplicand(gfc_batch &bt, size_t src)
 {
@@ -729,6 +747,11 @@ GFC_API int gfc_set(gfc_transform *t, uint32_t a)
 GFC_API int gfc_square_dup(gfc_transform *t, int dup)
 {
 	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_square(*t, dup ? DUP_ALL : DUP_NONE, 1); });
+}
+
+GFC_API int gfc_square_mul(gfc_transform *t, int32_t a)
+{
+	return guard([&] { GFC_NULLCHK(t); cudaSetDevice(t->device); op_square_mul(*t, a); });
 }
 
 GFC_API int gfc_init_multiplicand(gfc_transform *t, size_t src)

@@ -739,6 +739,32 @@ __global__ void __launch_bounds__(256) k_fixup(const Args a)
 	for (int i = 0; i < SEG / 4; ++i) p[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
 }
 
+// r_dst = m r_dst digit by digit, carrying inside 16-digit segments and leaving
+// the segment carries for k_fixup: the digit-times-scalar step of
+// transform::squareMul (src/transformCPUi32.h:774-797).  |digit m| < 2^62.
+__global__ void __launch_bounds__(256) k_mulscalar(const Args a, int32_t m)
+{
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	const size_t N = size_t(1) << a.n;
+	const size_t s = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (s >= N / SEG) return;
+	int4 *p = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(a.dst) * N + s * SEG);
+	int32_t dg[SEG];
+#pragma unroll
+	for (int i = 0; i < SEG / 4; ++i)
+	{
+		const int4 v = p[i];
+		dg[4 * i] = v.x; dg[4 * i + 1] = v.y; dg[4 * i + 2] = v.z; dg[4 * i + 3] = v.w;
+	}
+	int64_t c = 0;
+#pragma unroll
+	for (int i = 0; i < SEG; ++i) dg[i] = carry_wide(static_cast<int64_t>(dg[i]) * m + c, d.ck, c);
+#pragma unroll
+	for (int i = 0; i < SEG / 4; ++i) p[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
+	d.carry[s] = c;
+}
+
 // ------------------------------------------------------------------ utilities
 
 // reg[dst] = a (digit 0), 0 elsewhere, for every test of the launch.

@@ -177,6 +177,10 @@ class Transform:
     def squareDup(self, dup: bool):
         check(lib().gfc_square_dup(self._batch.handle, 1 if dup else 0))
 
+    def squareMul(self, a: int):
+        """r_0 = a r_0^2 (transform::squareMul, src/transform.h:60)."""
+        check(lib().gfc_square_mul(self._batch.handle, a))
+
     def initMultiplicand(self, src: int):
         check(lib().gfc_init_multiplicand(self._batch.handle, src))
 

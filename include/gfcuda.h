@@ -66,6 +66,10 @@ int gfc_set(gfc_transform *t, uint32_t a);
 /* r_0 = r_0^2, or 2 r_0^2 when dup != 0  (transform::squareDup, src/transform.h:59). */
 int gfc_square_dup(gfc_transform *t, int dup);
 
+/* r_0 = a r_0^2 for any int32 a  (transform::squareMul, src/transform.h:60;
+ * CPU reference src/transformCPUi32.h:870-874, 774-797). */
+int gfc_square_mul(gfc_transform *t, int32_t a);
+
 /* r_m = transform(r_src)  (transform::initMultiplicand, src/transform.h:61). */
 int gfc_init_multiplicand(gfc_transform *t, size_t src);
 

@@ -403,6 +403,35 @@ static void baseMod(gfo_t *t, rns4 *z, int dup)
 	}
 }
 
+/* baseModMul (src/transformCPUi32.h:774-797): digits times a, then carry. */
+static void baseModMul(gfo_t *t, rns4 *z, int32_t a)
+{
+	const size_t n = t->size_4;
+	const uint32_t b = t->b;
+	i128 f[4] = { 0, 0, 0, 0 };
+	for (size_t k = 0; k < n; ++k)
+		for (int l = 0; l < 4; ++l)
+		{
+			f[l] += (i128)to_int(z[k].r[0][l], P1) * a;
+			set_digit(&z[k], l, reduce(&f[l], b));
+		}
+	int64_t c[4]; for (int l = 0; l < 4; ++l) c[l] = (int64_t)f[l];
+	while ((c[0] | c[1] | c[2] | c[3]) != 0)
+	{
+		const int64_t c3 = c[3]; c[3] = c[2]; c[2] = c[1]; c[1] = c[0]; c[0] = -c3;
+		for (size_t k = 0; k < n; ++k)
+		{
+			for (int l = 0; l < 4; ++l)
+			{
+				i128 g = (i128)c[l] + to_int(z[k].r[0][l], P1);
+				set_digit(&z[k], l, reduce(&g, b));
+				c[l] = (int64_t)g;
+			}
+			if ((c[0] | c[1] | c[2] | c[3]) == 0) return;
+		}
+	}
+}
+
 /* ---------------- public C ABI (checker only) ---------------- */
 
 GFO_API void *gfo_create(uint32_t b, uint32_t n, size_t num_regs)
@@ -443,6 +472,14 @@ GFO_API void gfo_square_dup(void *h, int dup)
 	square_rec(t->z, t->wr, &t->wr[size_4], size_4 / 4, 1, 0);
 	backward0(t, t->z, size_4);
 	baseMod(t, t->z, dup);
+}
+
+/* squareMul (:870-874) */
+GFO_API void gfo_square_mul(void *h, int32_t a)
+{
+	gfo_t *t = (gfo_t *)h;
+	gfo_square_dup(h, 0);
+	baseModMul(t, t->z, a);
 }
 
 /* initMultiplicand (:876-886) */

@@ -49,6 +49,7 @@ def lib():
         L.gfo_destroy.argtypes = [ctypes.c_void_p]
         L.gfo_set.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
         L.gfo_square_dup.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.gfo_square_mul.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.gfo_init_multiplicand.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
         L.gfo_mul.argtypes = [ctypes.c_void_p]
         L.gfo_copy.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
@@ -153,6 +154,9 @@ class OracleTransform:
     def squareDup(self, dup: bool):
         lib().gfo_square_dup(self._h, 1 if dup else 0)
 
+    def squareMul(self, a: int):
+        lib().gfo_square_mul(self._h, a)
+
     def initMultiplicand(self, src: int):
         lib().gfo_init_multiplicand(self._h, src)
 
@@ -202,6 +206,9 @@ class RefTransform:
 
     def squareDup(self, dup: bool):
         ref_lib().ref_square_dup(self._h, 1 if dup else 0)
+
+    def squareMul(self, a: int):
+        ref_lib().ref_square_mul(self._h, a)
 
     def run_squarings(self, bits: np.ndarray):
         x = np.ascontiguousarray(bits, dtype=np.uint8)

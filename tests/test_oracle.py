@@ -94,3 +94,15 @@ def test_oracle_matches_reference_raw(oracle, n):
 def test_reference_rns_kat(oracle):
     _, res64, _, ok = oracle.quick(oracle.RefTransform(10**9, 9), 10**9, 9)
     assert res64 == RNS_KATS[9] and ok
+
+
+@needs_ref
+def test_oracle_square_mul_matches_reference(oracle):
+    rng = np.random.default_rng(77)
+    b, n = 1_000_000_006, 10
+    o, r = oracle.OracleTransform(b, n), oracle.RefTransform(b, n)
+    d = rng.integers(-(b // 2), b // 2, size=1 << n).astype(np.int32)
+    o.setInt(d); r.setInt(d)
+    for a in (3, 5, 123456789, 2):
+        o.squareMul(a); r.squareMul(a)
+        assert np.array_equal(o.raw(), r.raw())

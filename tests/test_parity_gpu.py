@@ -194,3 +194,24 @@ def test_batch_exponent_graph(oracle, plan):
         assert np.array_equal(canon(got0[i], b), canon(o.getInt(), b))
         o.copy(0, 1)
         assert np.array_equal(canon(got1[i], b), canon(o.getInt(), b))
+
+
+@pytest.mark.parametrize("plan", [None, 4])
+@pytest.mark.parametrize("b", [SMALL_B, LARGE_B, 1024])
+def test_square_mul(oracle, b, plan):
+    """transform::squareMul (prime mode): r <- a r^2 for small, large and negative a."""
+    n = 12
+    rng = np.random.default_rng(b % 97)
+    t, o = Transform(b, n), oracle.OracleTransform(b, n)
+    if plan is not None:
+        t.batch.set_plan(plan)
+    d = rand_digits(rng, b, 1 << n)
+    t.setInt(d); o.setInt(d)
+    for a in (3, 1, 2, -1, 0x7fffffff, -0x80000000 + 1, 12345, 0, 7):
+        if a == 0:
+            t.setInt(d); o.setInt(d)
+            continue
+        t.squareMul(a); o.squareMul(a)
+        g = t.getInt()
+        assert np.abs(g).max() <= b // 2 + 1
+        assert np.array_equal(canon(g, b), canon(o.getInt(), b)), f"a={a}"
