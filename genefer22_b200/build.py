@@ -43,7 +43,7 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, *(extra or []), "-o", LIB + ".tmp", *SOURCES, "-lcudart"]
+    cmd = [nvcc(), *NVCC_FLAGS, *(extra or []), "-cudart=static", "-o", LIB + ".tmp", *SOURCES]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
