@@ -339,6 +339,180 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ other workloads (not the default line)
+
+def _device_time(streams, launch_all, torch):
+    """Device milliseconds of launch_all() whose work spans several streams:
+    every stream waits for a start event on a common stream, which then
+    waits for every stream before the end event."""
+    s0 = torch.cuda.current_stream()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(s0)
+    for s in streams:
+        s.wait_event(start)
+    launch_all()
+    for s in streams:
+        e = torch.cuda.Event()
+        e.record(s)
+        s0.wait_event(e)
+    end.record(s0)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def _plain_rate(b: int, n: int, squarings: int) -> float:
+    """One test, one gfc_square_dup call per squaring (digit-squarings/s)."""
+    from genefer22_b200 import Transform
+    tr = Transform(int(b), n)
+    tr.set(3)
+    for _ in range(5):
+        tr.squareDup(False)
+    tr.sync()
+    t0 = time.perf_counter()
+    for i in range(squarings):
+        tr.squareDup(i % 2 == 1)
+    tr.sync()
+    return (1 << n) * squarings / (time.perf_counter() - t0)
+
+
+def run_uneven(args):
+    """256 tests, n from {12:40%,...,18:2%}, b log-uniform [1024, 2e9) clipped
+    to the per-n limits (seed 1004); one step = one Gerbicz-Li block of
+    1000 squarings of every test, the size classes' graphs in flight together."""
+    import torch
+    from genefer22_b200.autotune import Autotuner
+    from genefer22_b200.genefer import Job
+    from genefer22_b200.mixed import MixedBatch, uneven_tests
+    torch.cuda.set_device(0)
+    tests = uneven_tests(256, seed=1004)
+    nblk = args.warmup + 2 * args.steps + 2
+    jobs = [Job.prefix(b, n, nblk * BLOCK) for b, n in tests]
+    tuner = Autotuner(squarings=8, replays=3)
+    mb = MixedBatch(jobs, B=BLOCK, tuner=tuner)
+    for c in mb.classes:
+        c.prp.load()
+        c.prp.block_graph()
+    streams = [torch.cuda.ExternalStream(c.batch.stream) for c in mb.classes]
+    launch = lambda: [c.prp.block_graph().launch() for c in mb.classes]
+    for _ in range(args.warmup):
+        launch()
+    for c in mb.classes:
+        c.batch.sync()
+    mix_ms = [_device_time(streams, launch, torch) for _ in range(args.steps)]
+    # the same blocks with the classes one after another
+    seq_ms = []
+    for _ in range(args.steps):
+        t = 0.0
+        for c, s in zip(mb.classes, streams):
+            t += _device_time([s], lambda c=c: c.prp.block_graph().launch(), torch)
+        seq_ms.append(t)
+    digits = sum(1 << n for _, n in tests)
+    value = digits * BLOCK * args.steps / (sum(mix_ms) * 1e-3)
+    per_class = {}
+    plain_s = 0.0
+    for c in mb.classes:
+        pr = _plain_rate(c.batch.bases[0], c.n, 200 if c.n <= 16 else 60)
+        plain_s += len(c.index) * (1 << c.n) * BLOCK / pr
+        per_class[c.n] = {"tests": len(c.index), "plan_lr": c.batch.plan(),
+                          "rns_widths": {"2": int(np.sum(c.batch.widths() == 2)), "3": int(np.sum(c.batch.widths() == 3))},
+                          "tuned_us_per_squaring": {str(k): round(v, 2) for k, v in c.tune.us.items()},
+                          "plain_digit_sq_per_s": pr}
+    plain = digits * BLOCK / plain_s
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.mean(mix_ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "uneven batch of 256 tests, n 12..18 (40/20/15/10/8/5/2 %), b log-uniform "
+                                   "[1024,2e9) clipped per n, seed 1004, Gerbicz-Li block of 1000 squarings",
+                       "classes": per_class},
+            "sequential_classes": {"value": digits * BLOCK * args.steps / (sum(seq_ms) * 1e-3),
+                                   "ms_per_step": float(np.mean(seq_ms))},
+            "plain": {"value": plain, "what": "each test alone, one gfc_square_dup call per squaring"},
+            "mixed_over_plain": value / plain}
+    mb.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Poisson arrivals of tests with n uniform in 15..22 and b even uniform up
+    to the per-n limit, plus one n=23 test with b near 2.5e7 (seed 1005), an
+    80 GB device-memory budget, Gerbicz-Li block B = 1000.  Each request runs
+    the first 2..4 blocks of its test's exponent.  A first pass with every
+    request arriving at once measures the service rate; the arrival rate is
+    then 80 % of it."""
+    from genefer22_b200.autotune import Autotuner
+    from genefer22_b200.serve import Server, serve_requests
+    count = args.serve_requests
+    tuner = Autotuner(squarings=4, replays=2)
+    sat = serve_requests(count, rate=1e9, blocks=[2, 3, 4], B=BLOCK, seed=1005)
+    srv = Server(B=BLOCK, budget_bytes=80 * 10**9, tuner=tuner)
+    with Clocks(0) as ck0:
+        srv.run(sat, timeout_s=1800)
+    cap = srv.stats
+    rate = 0.8 * cap.completed / cap.seconds
+    reqs = serve_requests(count, rate=rate, blocks=[2, 3, 4], B=BLOCK, seed=1005)
+    srv = Server(B=BLOCK, budget_bytes=80 * 10**9, tuner=tuner)
+    with Clocks(0) as ck:
+        comps = srv.run(reqs, timeout_s=1800)
+    st = srv.stats
+    line = {"metric": METRIC, "value": st.rate, "unit": METRIC, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"serving: {count} Poisson requests n~U{{15..22}} + one n=23 b~2.5e7, "
+                                   "b even uniform up to the per-n limit, seed 1005, 80 GB budget, B=1000, "
+                                   "2..4 blocks per request",
+                       "arrival_rate_per_s": rate, "service_rate_per_s": cap.completed / cap.seconds},
+            "p50_time_to_residue_s": st.p50, "p99_time_to_residue_s": st.p99,
+            "p50_time_to_validated_s": st.p50_validated, "p99_time_to_validated_s": st.p99_validated,
+            "mean_queue_wait_s": st.mean_wait, "completed": st.completed, "gl_failures": st.gl_failures,
+            "pools_created": st.pools_created, "peak_budget_bytes": st.peak_bytes,
+            "saturated": {"value": cap.rate, "seconds": cap.seconds, "p50_s": cap.p50, "p99_s": cap.p99},
+            "per_n": {str(k): v for k, v in st.per_n.items()},
+            "clocks": ck.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_sizes(args):
+    """Per size n = 12..23: a batch (tests per launch as in serving pools) run as
+    graph-replayed blocks vs the plain path (one test, one call per squaring)."""
+    import torch
+    from genefer22_b200 import Batch
+    from genefer22_b200 import genefer as gf
+    from genefer22_b200.autotune import Autotuner
+    from genefer22_b200.mixed import b_limit
+    torch.cuda.set_device(0)
+    tuner = Autotuner(squarings=4, replays=2)
+    rng = np.random.default_rng(11)
+    out = {}
+    hbm, hbm_kind = peaks()
+    for n in range(12, 24):
+        count = {12: 256, 13: 128, 14: 64, 15: 64, 16: 64, 17: 16, 18: 8, 19: 4, 20: 2, 21: 2, 22: 1, 23: 1}[n]
+        lim = min(b_limit(n), 100_000_000 if n >= 16 else 2_000_000_000)
+        bs = [int(x) & ~1 for x in rng.integers(1_000_000, lim, size=count)]
+        bt = Batch(bs, n, num_regs=3)
+        tr = tuner.tune(bt)
+        blk = 200 if n <= 18 else 50
+        runner = gf.BatchPRP(bt, B=blk, exps=[gf.Job.prefix(b, n, 8 * blk).words_nbits() for b in bs])
+        runner.load()
+        bt.square_exp(runner.schedule()[0])
+        bt.gl_step()
+        g = runner.block_graph()
+        g.launch()
+        s = torch.cuda.ExternalStream(bt.stream)
+        ms = min(_device_time([s], g.launch, torch) for _ in range(3))
+        batched = count * (1 << n) * blk / (ms * 1e-3)
+        plain = _plain_rate(bs[0], n, 100 if n <= 18 else 30)
+        W = bt.widths()
+        sq_ms = ms / blk
+        alg_bytes = float(np.sum(16 * W * (1 << n)))
+        out[n] = {"tests": count, "plan_lr": tr.lr, "widths": sorted(set(int(w) for w in W)),
+                  "batched": batched, "plain": plain, "batched_over_plain": batched / plain,
+                  "us_per_batch_squaring": sq_ms * 1e3,
+                  "hbm_frac_16WN": alg_bytes / (sq_ms * 1e-3) / 1e9 / hbm}
+        g.close()
+        bt.close()
+    print(json.dumps({"metric": METRIC, "unit": METRIC, "workload": "sizes", "hbm_peak_gbs": hbm,
+                      "hbm_peak_kind": hbm_kind, "sizes": out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -347,11 +521,20 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="batch", choices=["batch", "uneven", "serve", "sizes"],
+                    help="batch: the default line; the others print their own line")
+    ap.add_argument("--serve-requests", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "uneven":
+        run_uneven(args)
+    elif args.workload == "serve":
+        run_serve(args)
+    elif args.workload == "sizes":
+        run_sizes(args)
     else:
         run_ours(args)
 

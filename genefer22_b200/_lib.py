@@ -50,6 +50,7 @@ SIGNATURES = {
     "gfc_batch_copy": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_size_t]),
     "gfc_batch_square": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_uint32]),
     "gfc_batch_set_exponent": (ctypes.c_int, [vp, ctypes.c_size_t, c_u32p, ctypes.c_uint64]),
+    "gfc_batch_assign": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_uint32]),
     "gfc_batch_set_pos": (ctypes.c_int, [vp, c_i64p]),
     "gfc_batch_get_pos": (ctypes.c_int, [vp, c_i64p]),
     "gfc_batch_square_exp": (ctypes.c_int, [vp, ctypes.c_uint32]),

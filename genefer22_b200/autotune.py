@@ -1,0 +1,120 @@
+"""Per size class choice of the squaring plan, by measurement.
+
+A plan is the split of the length-N transform: ``lr = 0`` keeps a whole test
+in one CTA's shared memory (n <= 14); ``lr >= 3`` runs the four-step form,
+2^lr-point column transforms (radix-16 register groups, 2^lr-point tiles in
+shared memory or registers) then 2^(n - lr)-point row transforms, the row
+pass carrying the pointwise product.  The prime set (RNS width, 2 or 3
+primes) is not a free choice: the narrowest set whose product bounds the
+convolution exactly is always the fastest (one plane less of every pass), so
+the engine takes it per test and the tuner reports it.
+
+The reference has no counterpart: genefer runs one test per transform with a
+fixed GPU kernel split chosen from n (src/transformGPU.h:945-1083).
+
+The tuner captures K squarings of each candidate plan into a CUDA graph,
+replays it, and keeps the fastest (device time per squaring, taken as the
+minimum over a few replays).  It squares register 0 of the batch in place, so
+tune a batch before loading its tests.  Results are cached per
+(n, test count, tests on the 3-prime set) in memory and, optionally, in a JSON
+file.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from ._lib import GfcError
+from .transform import Batch
+
+SMALL_MAX_LOGN = 14
+
+
+def candidates(n: int) -> List[int]:
+    """Plans the engine accepts for size n (it rejects the others with GFC_ERR_ARG)."""
+    out = [0] if n <= SMALL_MAX_LOGN else []
+    for lr in range(3, 11):
+        lc = n - lr
+        if 8 <= lc <= 13:
+            out.append(lr)
+    return out
+
+
+@dataclass
+class TuneResult:
+    n: int
+    count: int
+    wide: int                       # tests on the 3-prime set
+    lr: int                         # chosen plan
+    us: Dict[int, float] = field(default_factory=dict)   # plan -> microseconds per batch squaring
+
+    def key(self) -> str:
+        return key(self.n, self.count, self.wide)
+
+
+def key(n: int, count: int, wide: int) -> str:
+    return f"n{n}_c{count}_w{wide}"
+
+
+class Autotuner:
+    def __init__(self, cache_path: Optional[str] = None, squarings: int = 16, replays: int = 3):
+        self.cache_path = cache_path
+        self.squarings = int(squarings)
+        self.replays = int(replays)
+        self.cache: Dict[str, dict] = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                self.cache = json.load(f)
+
+    def _save(self):
+        if self.cache_path:
+            tmp = self.cache_path + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(self.cache, f, indent=1, sort_keys=True)
+            os.replace(tmp, self.cache_path)
+
+    def measure(self, bt: Batch, lr: int) -> float:
+        """Microseconds per batch squaring of plan lr (graph replay, device-bound)."""
+        bt.set_plan(lr)
+        K = self.squarings
+        g = bt.capture(lambda: bt.square(False, K))
+        try:
+            g.launch()
+            bt.sync()
+            best = float("inf")
+            for _ in range(self.replays):
+                t0 = time.perf_counter()
+                g.launch()
+                bt.sync()
+                best = min(best, time.perf_counter() - t0)
+        finally:
+            g.close()
+        return best / K * 1e6
+
+    def tune(self, bt: Batch, force: bool = False) -> TuneResult:
+        """Chooses and sets the fastest plan for bt (before its tests are loaded)."""
+        wide = int(np.count_nonzero(bt.widths() == 3))
+        k = key(bt.n, bt.count, wide)
+        if (not force) and (k in self.cache):
+            c = self.cache[k]
+            bt.set_plan(int(c["lr"]))
+            return TuneResult(bt.n, bt.count, wide, int(c["lr"]), {int(a): v for a, v in c["us"].items()})
+        us: Dict[int, float] = {}
+        for lr in candidates(bt.n):
+            try:
+                us[lr] = self.measure(bt, lr)
+            except GfcError:
+                continue
+        if not us:
+            raise GfcError(-1, f"no valid plan for n={bt.n}")
+        best = min(us, key=lambda lr: (us[lr], lr))
+        bt.set_plan(best)
+        bt.set(0)
+        self.cache[k] = {"lr": best, "us": {str(a): v for a, v in us.items()}}
+        self._save()
+        return TuneResult(bt.n, bt.count, wide, best, us)

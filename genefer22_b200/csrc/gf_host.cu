@@ -332,6 +332,7 @@ struct gfc_batch
 	std::vector<uint32_t *> ebits;
 	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };   // tests per prime set; d_tests lists set 0 first
 	int pending = -1;             // register whose segment carries are not yet absorbed (four-step)
+	uint64_t sets_version = 0;    // bumped when a test changes prime set (per-set launches change)
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
 
@@ -352,6 +353,8 @@ struct gfc_graph
 	cudaGraph_t graph = nullptr;
 	cudaGraphExec_t exec = nullptr;
 	uint64_t kernels = 0;         // kernel nodes recorded
+	uint64_t sets_version = 0;    // batch's sets_version at capture
+	bool per_set = false;         // recorded per-prime-set launches (single-CTA plan)
 	~gfc_graph()
 	{
 		cudaSetDevice(device);
@@ -885,6 +888,38 @@ GFC_API int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *w
 	});
 }
 
+GFC_API int gfc_batch_assign(gfc_batch *bt, size_t test, uint32_t b)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt);
+		check_test(*bt, test);
+		no_capture(*bt);
+		if ((b < 8) || (b >= (1u << 31))) fail(GFC_ERR_ARG, "assign: base b must satisfy 8 <= b < 2^31");
+		const int s = choose_set(b, bt->n);
+		if (s < 0) fail(GFC_ERR_RANGE, "assign: (b, n) is outside the exact range of the RNS prime sets");
+		cudaSetDevice(bt->device);
+		materialize(*bt);
+		GFC_CK(cudaStreamSynchronize(bt->stream));
+		if (s != bt->set[test]) bt->sets_version++;
+		bt->nset[bt->set[test]]--;
+		bt->b[test] = b;
+		bt->set[test] = s;
+		bt->nset[s]++;
+		bt->offset[0] = 0; bt->offset[1] = bt->nset[0];
+		std::vector<int32_t> tests;
+		for (int k = 0; k < 2; ++k)
+			for (size_t i = 0; i < bt->count; ++i)
+				if (bt->set[i] == k) tests.push_back(static_cast<int32_t>(i));
+		TestDesc &d = bt->h_desc[test];
+		d.b = b;
+		d.set = s;
+		d.ck = carry_constants(b, s);
+		GFC_CK(cudaMemcpy(bt->d_desc + test, &d, sizeof(TestDesc), cudaMemcpyHostToDevice));
+		GFC_CK(cudaMemcpy(bt->d_tests, tests.data(), bt->count * sizeof(int32_t), cudaMemcpyHostToDevice));
+		prepare_plan(*bt);
+	});
+}
+
 GFC_API int gfc_batch_set_pos(gfc_batch *bt, const int64_t *pos)
 {
 	return guard([&] {
@@ -1056,6 +1091,7 @@ GFC_API int gfc_batch_capture_end(gfc_batch *bt, gfc_graph **out)
 		bt->capturing = false;
 		std::unique_ptr<gfc_graph> g(new gfc_graph());
 		g->batch = bt; g->device = bt->device; g->stream = bt->stream;
+		g->sets_version = bt->sets_version; g->per_set = (bt->lr == 0);
 		// recorded launches are counted when the graph runs, not here
 		g->kernels = g_launches.load() - bt->capture_start;
 		g_launches.fetch_sub(g->kernels);
@@ -1070,6 +1106,8 @@ GFC_API int gfc_graph_launch(gfc_graph *g)
 	return guard([&] {
 		GFC_NULLCHK(g);
 		cudaSetDevice(g->device);
+		if ((g->batch != nullptr) && g->per_set && (g->batch->sets_version != g->sets_version))
+			fail(GFC_ERR_STATE, "graph_launch: a test changed prime set since capture; capture again");
 		if (g->batch != nullptr) materialize(*g->batch);
 		GFC_CK(cudaGraphLaunch(g->exec, g->stream));
 		g_launches.fetch_add(g->kernels);

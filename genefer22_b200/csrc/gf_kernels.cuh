@@ -140,9 +140,16 @@ __device__ __forceinline__ bool absorb(int32_t (&dg)[D], int64_t c, const CarryK
 }
 
 // Carry into segment s (16 digits) of a register with N / SEG segments.
-__device__ __forceinline__ int64_t carry_in(const TestDesc &d, size_t s, size_t nseg)
+// Takes the pending carry into segment s (negated across the wrap) and clears
+// it, so that a carry is absorbed exactly once even when the test sits out
+// later squarings of its batch (DUP_BITS, position below 0) while batch-wide
+// fix-ups keep running.
+__device__ __forceinline__ int64_t take_carry(const TestDesc &d, size_t s, size_t nseg)
 {
-	return (s == 0) ? -d.carry[nseg - 1] : d.carry[s - 1];
+	int64_t *const p = (s == 0) ? &d.carry[nseg - 1] : &d.carry[s - 1];
+	const int64_t c = *p;
+	if (c != 0) *p = 0;
+	return (s == 0) ? -c : c;
 }
 
 // Absorbs the pending carry of one segment held in shared memory (element i
@@ -426,7 +433,7 @@ __device__ __forceinline__ void col_fwd_body(const Args &a, const TestDesc &d, u
 		{
 			const int k = e / (S::CW / SEG), sg = e % (S::CW / SEG);
 			const size_t j0 = static_cast<size_t>(k) * C + c0 + sg * SEG;
-			fix_segment(d, dg + MP::addr(k, sg * SEG), 1, srcreg + j0, carry_in(d, j0 / SEG, nseg), a.err);
+			fix_segment(d, dg + MP::addr(k, sg * SEG), 1, srcreg + j0, take_carry(d, j0 / SEG, nseg), a.err);
 		}
 		__syncthreads();
 		for (int e = threadIdx.x; e < S::R * S::CW; e += blockDim.x)
@@ -615,7 +622,7 @@ __device__ __forceinline__ void col_fwd_reg_body(const Args &a, const TestDesc &
 		{
 			const int k = e / (T / SEG), s = e % (T / SEG);
 			const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
-			fix_segment(d, sm + k * (T + 1) + s * SEG, 1, srcreg + j0, carry_in(d, j0 / SEG, nseg), a.err);
+			fix_segment(d, sm + k * (T + 1) + s * SEG, 1, srcreg + j0, take_carry(d, j0 / SEG, nseg), a.err);
 		}
 		__syncthreads();
 #pragma unroll
@@ -724,7 +731,7 @@ __global__ void __launch_bounds__(256) k_fixup(const Args a)
 	const size_t nseg = N / SEG;
 	const size_t s = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
 	if (s >= nseg) return;
-	const int64_t cin = (s == 0) ? -d.carry[nseg - 1] : d.carry[s - 1];
+	const int64_t cin = take_carry(d, s, nseg);
 	if (cin == 0) return;
 	int4 *p = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(a.dst) * N + s * SEG);
 	int32_t dg[SEG];

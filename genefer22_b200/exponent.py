@@ -89,3 +89,40 @@ def chunk_sum(words: np.ndarray, nbits: int, B: int) -> int:
     for i in range(B - 1, -1, -1):
         res = (res << 1) + int(cs[i])
     return res
+
+
+def _int_to_words(v: int, nbits: int) -> np.ndarray:
+    nw = max(1, (int(nbits) + 31) // 32)
+    return np.frombuffer(int(v).to_bytes(4 * nw, "little"), dtype="<u4").astype(np.uint32)
+
+
+def prefix_words(b: int, n: int, bits: int) -> Tuple[np.ndarray, int, int]:
+    """The top ``bits`` bits of E = b^(2^n) without forming E: returns
+    (words of the prefix, its bit count, bit length of E).
+
+    E is bracketed by squaring lower and upper bounds truncated to bits + 64
+    bits (floor and ceiling); the prefix is exact when both bounds give the
+    same bit length and the same top bits, which fails only if E's bits below
+    the prefix are all 0 or all 1 for about 64 - n positions.  Then, and for
+    prefixes of (nearly) the whole exponent, E is computed in full."""
+    b, n, bits = int(b), int(n), int(bits)
+    P = bits + 64
+    lo = hi = b
+    e = 0
+    for _ in range(n):
+        lo, hi, e = lo * lo, hi * hi, 2 * e
+        s = lo.bit_length() - P
+        if s > 0:
+            lo >>= s
+            hi = -((-hi) >> s)
+            e += s
+    nb_lo, nb_hi = lo.bit_length() + e, hi.bit_length() + e
+    if (e > 0) and (nb_lo == nb_hi) and (nb_lo - bits - e >= 0):
+        sh = nb_lo - bits - e
+        if (lo >> sh) == (hi >> sh):
+            return _int_to_words(lo >> sh, bits), bits, nb_lo
+    words, nb = exponent_words(b, n)
+    if bits >= nb:
+        return words, nb, nb
+    v = words_to_int(words) >> (nb - bits)
+    return _int_to_words(v, bits), bits, nb

@@ -16,7 +16,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import gint
-from .exponent import B_GerbiczLi, bit, chunk_sum, exponent_words
+from .exponent import B_GerbiczLi, bit, chunk_sum, exponent_words, prefix_words
 from .transform import Batch, Transform
 
 
@@ -28,6 +28,31 @@ class Result:
     res64: int
     old64: int
     gl_ok: bool
+
+
+@dataclass
+class Job:
+    """One exponentiation 2^e mod b^(2^n)+1 as the PRP loop runs it: e is the
+    test's exponent E = b^(2^n) (``full``) or its top ``bits`` bits
+    (``prefix``), whose result is the state of the full test after ``bits``
+    squarings (src/genefer.h:505-549 stopped early)."""
+    b: int
+    n: int
+    words: np.ndarray
+    nbits: int
+
+    @classmethod
+    def full(cls, b: int, n: int) -> "Job":
+        w, nb = exponent_words(int(b), int(n))
+        return cls(int(b), int(n), w, nb)
+
+    def words_nbits(self):
+        return self.words, self.nbits
+
+    @classmethod
+    def prefix(cls, b: int, n: int, bits: int) -> "Job":
+        w, k, _ = prefix_words(int(b), int(n), int(bits))
+        return cls(int(b), int(n), w, k)
 
 
 # ------------------------------------------------------------------ one test
@@ -83,12 +108,52 @@ def _pad(words: np.ndarray, nwords: int) -> np.ndarray:
     return out
 
 
-class BatchPRP:
-    """Fermat PRP tests of every test of a Batch with a common block length B."""
+def _int_words(v: int) -> np.ndarray:
+    nw = max(1, (int(v).bit_length() + 31) // 32)
+    return np.frombuffer(int(v).to_bytes(4 * nw, "little"), dtype="<u4").astype(np.uint32)
 
-    def __init__(self, batch: Batch, B: Optional[int] = None):
+
+def gl_validate(bt: Batch, B: int, res: Sequence[int]) -> np.ndarray:
+    """genefer::GL (src/genefer.h:557-615) for every test of bt at once: reg0 =
+    the residue r, reg1 = d(t), res[i] = sum of the B-bit chunks of test i's
+    exponent; reg2 is overwritten.  Returns the per-test ok flags."""
+    bt.init_multiplicand(1)
+    bt.mul_into(0)                   # mul(1): r0 = r * d(t) = d(t+1)
+    bt.copy(2, 0)
+    bt.copy(0, 1)
+    bt.square(False, B)              # d(t)^(2^B)
+    bt.copy(1, 0)
+    rbits = max(1, max(int(r).bit_length() for r in res))
+    for i, r in enumerate(res):
+        w = np.zeros((rbits + 31) // 32, dtype=np.uint32)
+        rw = _int_words(r)
+        w[: rw.size] = rw
+        bt.set_exponent(i, w, rbits)
+    bt.set(1)
+    bt.square_exp(rbits)             # 2^res
+    bt.init_multiplicand(1)
+    bt.mul_into(0)                   # d(t)^(2^B) * 2^res
+    a = bt.get_all(0)
+    c = bt.get_all(2)
+    ok = np.zeros(bt.count, dtype=bool)
+    for i, b in enumerate(bt.bases):
+        ok[i] = gint.hash64(gint.unbalance(a[i], int(b))) == gint.hash64(gint.unbalance(c[i], int(b)))
+    return ok
+
+
+class BatchPRP:
+    """Fermat PRP tests of every test of a Batch with a common block length B.
+    ``exps`` (one (words, nbits) per test) replaces the tests' exponents
+    b^(2^n), e.g. by the prefixes of ``Job.prefix``."""
+
+    def __init__(self, batch: Batch, B: Optional[int] = None, exps: Optional[Sequence] = None):
         self.batch = batch
-        self.exps = [exponent_words(int(b), batch.n) for b in batch.bases]
+        if exps is None:
+            self.exps = [exponent_words(int(b), batch.n) for b in batch.bases]
+        else:
+            if len(exps) != batch.count:
+                raise ValueError("one exponent per test")
+            self.exps = [(np.asarray(w, dtype=np.uint32), int(nb)) for (w, nb) in exps]
         self.nbits = max(nb for _, nb in self.exps)
         self.B = int(B) if B else B_GerbiczLi(self.nbits)
         self._graph = None
@@ -134,42 +199,26 @@ class BatchPRP:
 
     def validate(self) -> np.ndarray:
         """genefer::GL for every test (src/genefer.h:557-615); returns ok flags."""
-        bt, B = self.batch, self.B
-        bt.init_multiplicand(1)
-        bt.mul_into(0)                   # mul(1): r0 = r * d(t) = d(t+1)
-        bt.copy(2, 0)
-        bt.copy(0, 1)
-        bt.square(False, B)              # d(t)^(2^B)
-        bt.copy(1, 0)
-        res = [chunk_sum(w, nb, B) for (w, nb) in self.exps]
-        rbits = max(1, max(r.bit_length() for r in res))
-        nw = (rbits + 31) // 32
-        for i, r in enumerate(res):
-            w = np.frombuffer(int(r).to_bytes(4 * nw, "little"), dtype="<u4").astype(np.uint32)
-            bt.set_exponent(i, w, rbits)
-        bt.set(1)
-        bt.square_exp(rbits)             # 2^res
-        bt.init_multiplicand(1)
-        bt.mul_into(0)                   # d(t)^(2^B) * 2^res
-        a = bt.get_all(0)
-        c = bt.get_all(2)
-        ok = np.zeros(bt.count, dtype=bool)
-        for i, b in enumerate(bt.bases):
-            ok[i] = gint.hash64(gint.unbalance(a[i], int(b))) == gint.hash64(gint.unbalance(c[i], int(b)))
-        return ok
+        return gl_validate(self.batch, self.B, [chunk_sum(w, nb, self.B) for (w, nb) in self.exps])
 
-    def run(self) -> List[Result]:
-        self.load()
-        self.run_prp()
+    def results(self, validate: bool = True) -> List[Result]:
+        """Residues of reg0 after run_prp (kept in ``canon``, canonical digits),
+        then (optionally) the GL check, which overwrites the registers."""
         bt = self.batch
         r0 = bt.get_all(0)
-        out = []
         canon = [gint.unbalance(r0[i], int(b)) for i, b in enumerate(bt.bases)]
-        ok = self.validate()
+        self.canon = canon
+        ok = self.validate() if validate else np.ones(bt.count, dtype=bool)
+        out = []
         for i, b in enumerate(bt.bases):
             is_prp, r64, o64 = gint.is_one(canon[i], int(b))
             out.append(Result(int(b), bt.n, is_prp, r64, o64, bool(ok[i])))
         return out
+
+    def run(self) -> List[Result]:
+        self.load()
+        self.run_prp()
+        return self.results()
 
 
 def quick_batch(bases: Sequence[int], n: int, B: Optional[int] = None, device: int = 0) -> List[Result]:

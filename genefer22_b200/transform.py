@@ -82,6 +82,11 @@ class Batch:
         w = np.ascontiguousarray(words, dtype=np.uint32)
         check(lib().gfc_batch_set_exponent(self._h, test, w.ctypes.data_as(c_u32p), nbits))
 
+    def assign(self, test: int, b: int):
+        """Slot `test` now holds a test of base b (registers unchanged)."""
+        check(lib().gfc_batch_assign(self._h, test, b))
+        self.bases[test] = b
+
     def set_pos(self, pos: Sequence[int]):
         p = np.ascontiguousarray(np.asarray(pos, dtype=np.int64))
         check(lib().gfc_batch_set_pos(self._h, p.ctypes.data_as(c_i64p)))

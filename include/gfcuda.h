@@ -131,6 +131,14 @@ int gfc_batch_square(gfc_batch *bt, int dup, uint32_t count);
  * and sets its bit position to nbits - 1. */
 int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *words, uint64_t nbits);
 
+/* Gives slot `test` a new base b (its prime set and carry constants follow);
+ * the slot's registers keep their contents until overwritten.  Synchronises.
+ * Used to admit a new test into a running batch.  No counterpart in the
+ * reference, which runs one test per transform.  With the single-CTA plan
+ * (n <= 14) a graph captured before a change of prime set is refused by
+ * gfc_graph_launch (GFC_ERR_STATE); four-step graphs stay valid. */
+int gfc_batch_assign(gfc_batch *bt, size_t test, uint32_t b);
+
 /* Sets every test's bit position (pos[i] < 0: the test has finished). */
 int gfc_batch_set_pos(gfc_batch *bt, const int64_t *pos);
 int gfc_batch_get_pos(gfc_batch *bt, int64_t *pos);
