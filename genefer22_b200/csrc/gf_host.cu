@@ -245,8 +245,8 @@ void col_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 		using S = ColShape<LR>;
 		if (prep) { set_smem(k_col_fwd<LR>, S::SMEM); set_smem(k_col_inv<LR>, S::SMEM); return; }
 		const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / S::CW), static_cast<unsigned>(grid_y));
-		if (inv) k_col_inv<LR><<<grid, FS_THREADS, S::SMEM, s>>>(a);
-		else k_col_fwd<LR><<<grid, FS_THREADS, S::SMEM, s>>>(a);
+		if (inv) k_col_inv<LR><<<grid, col_threads(LR), S::SMEM, s>>>(a);
+		else k_col_fwd<LR><<<grid, col_threads(LR), S::SMEM, s>>>(a);
 		after_launch();
 	}
 }
@@ -273,7 +273,7 @@ void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep)
 	using S = RowShape<LC>;
 	if (prep) { set_smem(k_row<LC>, S::SMEM); return; }
 	const dim3 grid(1u << (a.n - LC), static_cast<unsigned>(grid_y));
-	k_row<LC><<<grid, FS_THREADS, S::SMEM, s>>>(a);
+	k_row<LC><<<grid, row_threads(LC), S::SMEM, s>>>(a);
 	after_launch();
 }
 

@@ -402,6 +402,11 @@ struct RowShape
 
 constexpr int FS_THREADS = 256;
 
+// Threads per CTA: a shared-memory tile that leaves room for one or two CTAs
+// on an SM gets more threads, so that every SM still holds 32 warps.
+__host__ __device__ constexpr int col_threads(int lr) { return (lr >= 9) ? 1024 : ((lr == 8) ? 512 : FS_THREADS); }
+__host__ __device__ constexpr int row_threads(int lc) { return (lc >= 13) ? 512 : FS_THREADS; }
+
 template <int SET, int LR>
 __device__ __forceinline__ void col_fwd_body(const Args &a, const TestDesc &d, uint32_t *sm)
 {
@@ -556,7 +561,7 @@ __device__ __forceinline__ void col_inv_body(const Args &a, const TestDesc &d, b
 
 // Columns: tile of CW columns x R rows; first log2 R forward stages.
 template <int LR>
-__global__ void __launch_bounds__(FS_THREADS) k_col_fwd(const Args a)
+__global__ void __launch_bounds__(col_threads(LR)) k_col_fwd(const Args a)
 {
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
@@ -569,7 +574,7 @@ __global__ void __launch_bounds__(FS_THREADS) k_col_fwd(const Args a)
 
 // Rows: the last log2 C forward stages, pointwise, first inverse stages.
 template <int LC>
-__global__ void __launch_bounds__(FS_THREADS) k_row(const Args a)
+__global__ void __launch_bounds__(row_threads(LC)) k_row(const Args a)
 {
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
@@ -582,7 +587,7 @@ __global__ void __launch_bounds__(FS_THREADS) k_row(const Args a)
 
 // Columns: last log2 R inverse stages, CRT, carry inside 16-digit segments.
 template <int LR>
-__global__ void __launch_bounds__(FS_THREADS) k_col_inv(const Args a)
+__global__ void __launch_bounds__(col_threads(LR)) k_col_inv(const Args a)
 {
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
