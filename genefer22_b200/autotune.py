@@ -1,7 +1,9 @@
 """Per size class choice of the squaring plan, by measurement.
 
 A plan is the split of the length-N transform: ``lr = 0`` keeps a whole test
-in one CTA's shared memory (n <= 14); ``lr >= 3`` runs the four-step form,
+in one CTA's shared memory (n <= 14); ``lr = 1`` keeps it in the shared
+memory of a thread-block cluster of 2^(n-13) CTAs (15 <= n <= 17); ``lr >= 3``
+runs the four-step form,
 2^lr-point column transforms (radix-16 register groups, 2^lr-point tiles in
 shared memory or registers) then 2^(n - lr)-point row transforms, the row
 pass carrying the pointwise product.  The prime set (RNS width, 2 or 3
@@ -35,9 +37,14 @@ from .transform import Batch
 SMALL_MAX_LOGN = 14
 
 
+PLAN_CLUSTER = 1
+
+
 def candidates(n: int) -> List[int]:
     """Plans the engine accepts for size n (it rejects the others with GFC_ERR_ARG)."""
     out = [0] if n <= SMALL_MAX_LOGN else []
+    if 15 <= n <= 17:
+        out.append(PLAN_CLUSTER)
     for lr in range(3, 11):
         lc = n - lr
         if 8 <= lc <= 13:

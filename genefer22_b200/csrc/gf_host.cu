@@ -291,8 +291,56 @@ void launch_row(int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
 	}
 }
 
+// Cluster-resident squaring (k_cluster): `prep` raises the shared-memory limit,
+// allows 16-CTA clusters and returns in *max_out how many clusters fit on the
+// device at once; otherwise launches a persistent grid of
+// min(ntests, max_active) clusters over the tests a.tests[0 .. ntests-1].
+template <int LQ>
+void cluster_t(const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
+{
+	using S = ClusterShape<LQ>;
+	auto kern = k_cluster<LQ>;
+	cudaLaunchConfig_t cfg = {};
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeClusterDimension;
+	at[0].val.clusterDim.x = S::Q; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+	cfg.blockDim = dim3(S::T);
+	cfg.dynamicSmemBytes = S::SMEM;
+	cfg.attrs = at; cfg.numAttrs = 1;
+	if (prep)
+	{
+		set_smem(kern, S::SMEM);
+		if (S::Q > 8) GFC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+		cfg.gridDim = dim3(S::Q);
+		int m = 0;
+		GFC_CK(cudaOccupancyMaxActiveClusters(&m, kern, &cfg));
+		if (m < 1) fail(GFC_ERR_CUDA, "cluster plan: no cluster of this size fits on the device");
+		*max_out = m;
+		return;
+	}
+	const int ncl = (ntests < max_active) ? ntests : max_active;
+	cfg.gridDim = dim3(static_cast<unsigned>(ncl * S::Q));
+	cfg.stream = s;
+	GFC_CK(cudaLaunchKernelEx(&cfg, kern, a, ntests));
+	after_launch();
+}
+
+void launch_cluster_lq(int lq, const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
+{
+	switch (lq)
+	{
+		case 2: cluster_t<2>(a, ntests, max_active, s, prep, max_out); break;
+		case 3: cluster_t<3>(a, ntests, max_active, s, prep, max_out); break;
+		case 4: cluster_t<4>(a, ntests, max_active, s, prep, max_out); break;
+		default: fail(GFC_ERR_ARG, "cluster plan needs 15 <= n <= 17");
+	}
+}
+
+constexpr int PLAN_CLUSTER = 1;   // plan code of the cluster-resident squaring
+
 bool plan_valid(int n, int lr)
 {
+	if (lr == PLAN_CLUSTER) return (n >= 13 + 2) && (n <= 13 + 4);
 	if (lr == 0) return (n >= 10) && (n <= SMALL_MAX_LOGN);
 	const int lc = n - lr;
 	return (lr >= 3) && (lr <= 10) && (lc >= 8) && (lc <= 13) && ((lr <= 4) || (col_width(lr) <= (1 << lc)));
@@ -333,6 +381,8 @@ struct gfc_batch
 	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };   // tests per prime set; d_tests lists set 0 first
 	int pending = -1;             // register whose segment carries are not yet absorbed (four-step)
 	uint64_t sets_version = 0;    // bumped when a test changes prime set (per-set launches change)
+	int cluster = 0;              // log2 CTAs per cluster when squarings use k_cluster, else 0
+	int cluster_max = 0;          // clusters of k_cluster resident at once
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
 
@@ -407,11 +457,18 @@ void launch_small(const gfc_batch &bt, const Args &a0, cudaStream_t s, bool prep
 	}
 }
 
+// Cluster-resident squarings: one persistent launch over all tests.
+void launch_cluster(gfc_batch &bt, const Args &a, cudaStream_t s)
+{
+	launch_cluster_lq(bt.cluster, a, static_cast<int>(bt.count), bt.cluster_max, s, false, nullptr);
+}
+
 // Raises shared-memory limits of the kernels the current plan uses.
 void prepare_plan(gfc_batch &bt)
 {
 	Args a{};
 	a.n = bt.n;
+	if (bt.cluster > 0) launch_cluster_lq(bt.cluster, a, 0, 0, nullptr, true, &bt.cluster_max);
 	if (bt.lr == 0) launch_small(bt, a, nullptr, true);
 	else
 	{
@@ -459,6 +516,19 @@ void fourstep(gfc_batch &bt, Args a)
 void op_square(gfc_batch &bt, int dup_mode, uint32_t count)
 {
 	if (count == 0) return;
+	if (bt.cluster > 0)
+	{
+		// digits stay in shared memory for all `count` squarings; carries
+		// pending on register 0 are absorbed when a test is loaded
+		if ((bt.pending >= 0) && (bt.pending != 0)) materialize(bt);
+		Args a = make_args(bt);
+		a.op = OP_SQUARE; a.dup_mode = dup_mode; a.src = 0; a.dst = 0;
+		a.count = static_cast<int>(count);
+		a.fix = (bt.pending == 0) ? 1 : 0;
+		launch_cluster(bt, a, bt.stream);
+		bt.pending = -1;
+		return;
+	}
 	if ((bt.pending >= 0) && ((bt.lr == 0) || (bt.pending != 0))) materialize(bt);
 	Args a = make_args(bt);
 	a.op = OP_SQUARE; a.dup_mode = dup_mode; a.src = 0; a.dst = 0;
@@ -536,7 +606,16 @@ void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
 		for (uint32_t r = 0; r < reps; ++r)
 		{
 			GFC_CK(cudaEventRecord(ev[0], bt.stream));
-			if (bt.lr == 0)
+			if (bt.cluster > 0)
+			{
+				a.fix = (bt.pending == 0) ? 1 : 0;
+				launch_cluster(bt, a, bt.stream);
+				bt.pending = -1;
+				GFC_CK(cudaEventRecord(ev[1], bt.stream));
+				GFC_CK(cudaEventSynchronize(ev[1]));
+				acc[0] += span(0, 1);
+			}
+			else if (bt.lr == 0)
 			{
 				launch_small(bt, a, bt.stream, false);
 				GFC_CK(cudaEventRecord(ev[1], bt.stream));
@@ -557,7 +636,7 @@ void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
 				acc[1] += span(0, 1); acc[2] += span(1, 2); acc[3] += span(2, 3);
 			}
 		}
-		if (bt.lr != 0)
+		if ((bt.lr != 0) && (bt.cluster == 0))
 		{
 			GFC_CK(cudaEventRecord(ev[3], bt.stream));
 			materialize(bt);
@@ -1040,12 +1119,25 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 		cudaSetDevice(bt->device);
 		materialize(*bt);
 		GFC_CK(cudaStreamSynchronize(bt->stream));
-		bt->lr = lr;
+		if (lr == PLAN_CLUSTER)
+		{
+			// products keep the default four-step plan
+			bt->cluster = bt->n - ClusterShape<2>::LC;
+			bt->lr = default_plan(bt->n);
+		}
+		else
+		{
+			bt->cluster = 0;
+			bt->lr = lr;
+		}
 		prepare_plan(*bt);
 	});
 }
 
-GFC_API int gfc_batch_plan(const gfc_batch *bt) { return (bt == nullptr) ? GFC_ERR_ARG : bt->lr; }
+GFC_API int gfc_batch_plan(const gfc_batch *bt)
+{
+	return (bt == nullptr) ? GFC_ERR_ARG : ((bt->cluster > 0) ? PLAN_CLUSTER : bt->lr);
+}
 
 GFC_API int gfc_batch_widths(const gfc_batch *bt, int32_t *w)
 {

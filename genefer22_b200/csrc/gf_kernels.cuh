@@ -20,6 +20,7 @@
 #pragma once
 
 #include <type_traits>
+#include <cooperative_groups.h>
 #include "gf_ntt.cuh"
 
 namespace gfc {
@@ -373,6 +374,190 @@ __global__ void __launch_bounds__(SmallShape<SET, LOGN>::T, SmallShape<SET, LOGN
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.x];
 	small_body<SET, LOGN>(a, t, a.desc[t], sm);
+}
+
+// ------------------------------------------------------------------ k_cluster
+
+// One test per thread-block cluster of Q = 2^LQ CTAs, resident in shared
+// memory for many squarings.  The test is the four-step matrix of Q rows of
+// C = 2^13 digits; CTA q holds row q (digits q C .. q C + C - 1).  Per
+// squaring: the Q-point column transforms (stages 0 .. LQ-1, base 1) read and
+// write the Q rows through distributed shared memory, each CTA transforms its
+// row (stages LQ .. n-1 with base 2^LQ + q, pointwise square, inverse), the
+// inverse column transforms fold in the normalisation, and every thread turns
+// 16 consecutive digits of its row into balanced base-b digits (CRT + carry);
+// the carry out of each 16-digit segment enters the next one (across CTAs,
+// and negated from the last segment to the first: b^N = -1) before the next
+// squaring.  Digits stay in registers between squarings; global memory is
+// read when a test starts and written when it ends.  A persistent grid of
+// clusters takes tests t = cluster, cluster + clusters, ...
+template <int LQ>
+struct ClusterShape
+{
+	static constexpr int Q = 1 << LQ;
+	static constexpr int LC = 13;
+	static constexpr int C = 1 << LC;
+	static constexpr int PC = C + C / 32;                 // padded plane (RowMap)
+	static constexpr int T = 512;
+	static constexpr int D = C / T;                       // digits per thread
+	static constexpr size_t SMEM = size_t(WMAX) * PC * 4 + size_t(T) * 8;
+	static_assert(D == SEG, "one carry segment per thread");
+};
+
+// Distributed shared memory by 32-bit shared::cluster addresses: the word at
+// shared-memory address `a` of this CTA, in the CTA of cluster rank `rank`.
+__device__ __forceinline__ uint32_t dsm_addr(uint32_t a, uint32_t rank)
+{
+	uint32_t r;
+	asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+	return r;
+}
+__device__ __forceinline__ uint32_t dsm_ld(uint32_t a)
+{
+	uint32_t v;
+	asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+	return v;
+}
+__device__ __forceinline__ void dsm_st(uint32_t a, uint32_t v)
+{
+	asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+
+// Q-point column transforms of the columns q C/Q .. (q+1) C/Q - 1, all planes.
+template <int SET, int LQ, bool INV>
+__device__ __forceinline__ void cluster_cols(uint32_t *sm, int q, const Tables &tab)
+{
+	using S = ClusterShape<LQ>;
+	constexpr int Q = S::Q, CQ = S::C / Q;
+	using MP = RowMap<S::LC>;
+	const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+#pragma unroll 1
+	for (int j = threadIdx.x; j < CQ; j += S::T)
+	{
+		const uint32_t off = base + 4u * static_cast<uint32_t>(MP::addr(q * CQ + j, 0));
+		for_planes<SET>([&](auto PLc) {
+			constexpr int PL = decltype(PLc)::value;
+			using Z = ZS<SET, PL>;
+			const uint32_t a = off + 4u * PL * S::PC;
+			uint32_t x[Q];
+#pragma unroll
+			for (int k = 0; k < Q; ++k) x[k] = dsm_ld(dsm_addr(a, k));
+			if constexpr (!INV) fwd_reg<Z, LQ>(Z{}, x, 1u, tab.fw[PL]);
+			else inv_reg<Z, LQ>(Z{}, x, 1u, tab.iv[PL], true, __ldg(&tab.fw[PL][0]), __ldg(&tab.iv[PL][0]));
+#pragma unroll
+			for (int k = 0; k < Q; ++k) dsm_st(dsm_addr(a, k), x[k]);
+		});
+	}
+}
+
+// One test of prime set SET on this cluster: `count` squarings (fewer when
+// the exponent runs out), from register src to register dst.
+template <int SET, int LQ>
+__device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDesc &d, uint32_t *sm, int q)
+{
+	namespace cg = cooperative_groups;
+	using S = ClusterShape<LQ>;
+	constexpr int Q = S::Q, C = S::C, PC = S::PC, T = S::T, D = S::D, W = PrimeSet<SET>::W;
+	using MP = RowMap<S::LC>;
+	int64_t *const sc = reinterpret_cast<int64_t *>(sm + WMAX * PC);
+	cg::cluster_group cl = cg::this_cluster();
+	const int tid = threadIdx.x;
+	const Tables &tab = a.tab[SET];
+	const size_t N = size_t(C) * Q;
+	const size_t nseg = N / SEG;
+
+	// Every CTA of the cluster reads the position once, before the first
+	// cluster barrier, so that all take the same number of squarings.
+	const int64_t pos0 = (a.dup_mode == DUP_BITS) ? a.pos[t] : 0;
+	int iters = a.count;
+	if (a.dup_mode == DUP_BITS) iters = (pos0 + 1 < iters) ? static_cast<int>((pos0 < 0) ? 0 : pos0 + 1) : iters;
+
+	int32_t dg[D];
+	{
+		const size_t j0 = static_cast<size_t>(q) * C + static_cast<size_t>(tid) * D;
+		const int4 *src = reinterpret_cast<const int4 *>(d.regs + static_cast<size_t>(a.src) * N + j0);
+#pragma unroll
+		for (int i = 0; i < D / 4; ++i)
+		{
+			const int4 v = src[i];
+			dg[4 * i] = v.x; dg[4 * i + 1] = v.y; dg[4 * i + 2] = v.z; dg[4 * i + 3] = v.w;
+		}
+		if (a.fix)
+		{
+			const int64_t cin = take_carry(d, j0 / SEG, nseg);
+			if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
+		}
+	}
+
+	for (int it = 0; it < iters; ++it)
+	{
+		const bool dup = (a.dup_mode == DUP_BITS) ? exp_bit(d.ebits, pos0 - it) : (a.dup_mode == DUP_ALL);
+		for_planes<SET>([&](auto PLc) {
+			constexpr int PL = decltype(PLc)::value;
+			using Z = ZS<SET, PL>;
+#pragma unroll
+			for (int i = 0; i < D; ++i) sm[PL * PC + MP::addr(tid * D + i, 0)] = Z::from_int(dg[i]);
+		});
+		cl.sync();
+		cluster_cols<SET, LQ, false>(sm, q, tab);
+		cl.sync();
+		row_core<SET, S::LC, MP>(sm, PC, 0, (1u << LQ) + static_cast<uint32_t>(q), tab, nullptr, 0, OP_SQUARE);
+		cl.sync();
+		cluster_cols<SET, LQ, true>(sm, q, tab);
+		cl.sync();
+		int64_t c = 0;
+#pragma unroll
+		for (int i = 0; i < D; ++i)
+		{
+			uint32_t x[3];
+#pragma unroll
+			for (int pl = 0; pl < W; ++pl) x[pl] = sm[pl * PC + MP::addr(tid * D + i, 0)];
+			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
+		}
+		sc[tid] = c;
+		cl.sync();
+		int64_t cin;
+		if (tid > 0) cin = sc[tid - 1];
+		else
+		{
+			const uint32_t qp = (q == 0) ? Q - 1 : q - 1;
+			const uint32_t ra = dsm_addr(static_cast<uint32_t>(__cvta_generic_to_shared(sc + T - 1)), qp);
+			const uint64_t lo = dsm_ld(ra), hi = dsm_ld(ra + 4);
+			cin = static_cast<int64_t>(lo | (hi << 32));
+			if (q == 0) cin = -cin;
+		}
+		if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
+	}
+
+	{
+		const size_t j0 = static_cast<size_t>(q) * C + static_cast<size_t>(tid) * D;
+		int4 *dst = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(a.dst) * N + j0);
+#pragma unroll
+		for (int i = 0; i < D / 4; ++i) dst[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
+	}
+	if ((tid == 0) && (q == 0) && (a.dup_mode == DUP_BITS)) a.pos[t] = (pos0 - iters < -1) ? -1 : pos0 - iters;
+}
+
+// Persistent grid of clusters over the tests a.tests[0 .. ntests-1], of
+// either prime set.
+template <int LQ>
+__global__ void __launch_bounds__(ClusterShape<LQ>::T, 2) k_cluster(const Args a, int ntests)
+{
+	namespace cg = cooperative_groups;
+	using S = ClusterShape<LQ>;
+	extern __shared__ __align__(16) uint32_t sm[];
+	cg::cluster_group cl = cg::this_cluster();
+	const int q = static_cast<int>(cl.block_rank());
+	const int ncl = gridDim.x / S::Q, cid = blockIdx.x / S::Q;
+	for (int ti = cid; ti < ntests; ti += ncl)
+	{
+		const int t = a.tests[ti];
+		const TestDesc &d = a.desc[t];
+		if (d.set == 0) cluster_test<0, LQ>(a, t, d, sm, q); else cluster_test<1, LQ>(a, t, d, sm, q);
+		// the next test's first shared-memory writes follow this barrier, after
+		// every CTA has read this test's last carries
+		cl.sync();
+	}
 }
 
 // ------------------------------------------------------------------ four-step

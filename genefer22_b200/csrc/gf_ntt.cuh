@@ -39,6 +39,37 @@ __device__ __forceinline__ void bfly_gs(const Z &z, uint32_t &a, uint32_t &b, ui
 	b = z.mul(t, wi);
 }
 
+// The twiddles of one radix-2^r group: w[2^t - 1 + sb] = tw[(tbase << t) + sb]
+// for stage t < r of the group and sb < 2^t.  The 2^t words of stage t are
+// consecutive and start at a multiple of 2^t words, so stages t >= 2 load as
+// 16-byte vectors and stage 1 as one 8-byte vector (root tables start on
+// 32-byte boundaries).
+template <int r>
+__device__ __forceinline__ void load_twiddles(uint32_t (&w)[(1 << r) - 1], uint32_t tbase, const uint32_t *__restrict__ tw)
+{
+#pragma unroll
+	for (int t = 0; t < r; ++t)
+	{
+		const uint32_t *p = tw + (static_cast<size_t>(tbase) << t);
+		if (t >= 2)
+		{
+#pragma unroll
+			for (int v = 0; v < (1 << t) / 4; ++v)
+			{
+				const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p) + v);
+				w[(1 << t) - 1 + 4 * v] = u.x; w[(1 << t) + 4 * v] = u.y;
+				w[(1 << t) + 1 + 4 * v] = u.z; w[(1 << t) + 2 + 4 * v] = u.w;
+			}
+		}
+		else if (t == 1)
+		{
+			const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+			w[1] = u.x; w[2] = u.y;
+		}
+		else w[0] = __ldg(p);
+	}
+}
+
 // r forward stages on 2^r registers.  Stage t of the group uses the table
 // entries (tbase << t) + sb, sb < 2^t, with tbase = (base << sigma) + blk.
 // All 2^r - 1 roots are loaded before the first butterfly.
@@ -46,10 +77,7 @@ template <class Z, int r>
 __device__ __forceinline__ void fwd_reg(const Z &z, uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ tw)
 {
 	uint32_t w[(1 << r) - 1];
-#pragma unroll
-	for (int t = 0; t < r; ++t)
-#pragma unroll
-		for (int sb = 0; sb < (1 << t); ++sb) w[(1 << t) - 1 + sb] = __ldg(&tw[(tbase << t) + sb]);
+	load_twiddles<r>(w, tbase, tw);
 #pragma unroll
 	for (int t = 0; t < r; ++t)
 	{
@@ -71,10 +99,7 @@ __device__ __forceinline__ void inv_reg(const Z &z, uint32_t (&x)[1 << r], uint3
 										bool norm, uint32_t c_norm, uint32_t k_norm)
 {
 	uint32_t w[(1 << r) - 1];
-#pragma unroll
-	for (int t = 0; t < r; ++t)
-#pragma unroll
-		for (int sb = 0; sb < (1 << t); ++sb) w[(1 << t) - 1 + sb] = __ldg(&twi[(tbase << t) + sb]);
+	load_twiddles<r>(w, tbase, twi);
 #pragma unroll
 	for (int t = r - 1; t >= 0; --t)
 	{

@@ -164,8 +164,10 @@ int gfc_batch_get_all(gfc_batch *bt, size_t reg, int32_t *out);
 int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
 
 /* Kernel plan.  lr = 0: one CTA per test with the state in shared memory
- * (n <= 14); lr > 0: four-step with R = 2^lr rows (3 <= lr <= 10,
- * 8 <= n - lr <= 13).  gfc_batch_plan reads the current plan. */
+ * (n <= 14); lr = 1: squarings by one thread-block cluster per test with the
+ * state in the cluster's shared memory (15 <= n <= 17; products use the
+ * default four-step plan); lr >= 3: four-step with R = 2^lr rows
+ * (lr <= 10, 8 <= n - lr <= 13).  gfc_batch_plan reads the current plan. */
 int gfc_batch_set_plan(gfc_batch *bt, int lr);
 int gfc_batch_plan(const gfc_batch *bt);
 
