@@ -14,9 +14,10 @@ between two blocks with x = d = 1, so the d update that opens its first block
 leaves d = 1, as genefer starts (src/genefer.h:492-497); its exponent is
 padded with leading zero bits to a whole number of blocks.  When a test's
 last block ends, its x and d(t) are read back, the residue is reported
-(``residue_at``), the slot is freed, and x and d(t) go to a validator thread
-that runs genefer's Gerbicz-Li check (src/genefer.h:557-615) for several
-finished tests of one size at once (``validated_at``).
+(``residue_at``), the slot is freed, and x and d(t) go to the validator
+thread of that size, which runs genefer's Gerbicz-Li check
+(src/genefer.h:557-615) for several finished tests at once on a batch of its
+own (``validated_at``).
 
 Pools are created while the device-memory budget allows (per slot:
 registers, transform planes, multiplicand, carries and room for the longest
@@ -332,23 +333,22 @@ class Server:
                 self.vqueue[pool.n].append((act.comp, job, x, d))
             self.cv.notify_all()
 
-    # -------------------------------------------------------- validator
-    def _validator(self):
-        batches: Dict[int, Batch] = {}
+    # -------------------------------------------------------- validators
+    def _validator(self, n: int):
+        """Gerbicz-Li checks of finished tests of size n, up to validate_group
+        at once, on a batch and stream of its own."""
+        bt: Optional[Batch] = None
+        q = self.vqueue[n]
         try:
             while True:
                 with self.cv:
-                    while not any(self.vqueue.values()) and not self._stop_validator:
+                    while not q and not self._stop_validator:
                         self.cv.wait(0.01)
-                    if not any(self.vqueue.values()):
+                    if not q:
                         break
-                    n = min((q[0][0].residue_at, n) for n, q in self.vqueue.items() if q)[1]
-                    q = self.vqueue[n]
                     group = [q.popleft() for _ in range(min(len(q), self.validate_group))]
-                bt = batches.get(n)
                 if bt is None:
                     bt = Batch([1024] * self.validate_group, n, num_regs=NUM_REGS, device=self.device)
-                    batches[n] = bt
                 zero = np.zeros(1 << n, dtype=np.int32)
                 res = []
                 for i in range(self.validate_group):
@@ -374,7 +374,7 @@ class Server:
                 self.errors.append(e)
                 self.cv.notify_all()
         finally:
-            for bt in batches.values():
+            if bt is not None:
                 bt.close()
 
     def _validator_bytes(self, ns: Sequence[int]) -> int:
@@ -409,9 +409,10 @@ class Server:
                 with Batch([1024] * max(1, int(self.capacity(n))), n, num_regs=NUM_REGS, device=self.device) as bt:
                     self.tuner.tune(bt)
         self._t0 = time.perf_counter()
-        vth = threading.Thread(target=self._validator, name="validator", daemon=True) if self.validate else None
-        if vth is not None:
-            vth.start()
+        vths = [threading.Thread(target=self._validator, args=(n,), name=f"validator-n{n}", daemon=True)
+                for n in ns] if self.validate else []
+        for v in vths:
+            v.start()
         k = 0
         deadline = timeout_s
         try:
@@ -445,8 +446,8 @@ class Server:
             self._stop_validator = True
             with self.cv:
                 self.cv.notify_all()
-        if vth is not None:
-            vth.join(timeout=max(1.0, deadline - self.clock() + 60))
+        for v in vths:
+            v.join(timeout=max(1.0, deadline - self.clock() + 60))
         for p in list(self.pools):
             p.thread.join(timeout=5)
         self.budget.limit += vbytes

@@ -214,13 +214,20 @@ class Transform:
     def getCacheSize(self) -> int:
         return int(lib().gfc_get_cache_size(self._batch.handle))
 
+    def contextSize(self, num_regs: int) -> int:
+        """Bytes of saveContext(num_regs); num_regs 0 means every register, as
+        in the reference's readContext / saveContext (src/transformGPU.h:1127-1150)."""
+        return int(lib().gfc_context_size(self._batch.handle, num_regs or self._batch.num_regs))
+
     def saveContext(self, num_regs: int) -> bytes:
+        num_regs = num_regs or self._batch.num_regs
         size = int(lib().gfc_context_size(self._batch.handle, num_regs))
         buf = ctypes.create_string_buffer(size)
         check(lib().gfc_save_context(self._batch.handle, buf, size, num_regs))
         return buf.raw
 
     def readContext(self, data: bytes, num_regs: int) -> bool:
+        num_regs = num_regs or self._batch.num_regs
         buf = ctypes.create_string_buffer(bytes(data), len(data))
         rc = lib().gfc_read_context(self._batch.handle, buf, len(data), num_regs)
         if rc == -5:
