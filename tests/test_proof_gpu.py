@@ -83,3 +83,38 @@ def test_wrong_certificate_fails(tmp_path):
         f.write_i32(v); f.write_i32(B); pf.write_gint(f, g, b); f.write_mpz(p2 + 1); f.write_crc32()
     ck = pf.check(Transform(b, n, 4), b, n, str(tmp_path / "b.cert"))
     assert ck is not None and ck != s.ckey
+
+
+# ------------------------------------------------------------------ deterministic test (mode "prime")
+
+from genefer22_b200 import genefer as gf
+from genefer22_b200 import prime as pm
+
+
+def test_prime_on_gpu():
+    assert pm.prime(Transform(824, 10), 824, 10).is_prime is True
+    assert pm.prime(Transform(16, 10), 16, 10).is_prime is False      # 2^4096 + 1: probable prime to base 2, composite
+    assert pm.prime(Transform(150, 11), 150, 11).is_prime is True
+    assert pm.prime(Transform(826, 10), 826, 10).is_prime is False
+
+
+def test_prp_scan_then_prove():
+    """Every even b in [8, 1000) at n = 10 that is not a power of two (the
+    bases genefer accepts, src/main.cpp:249-253: base 2 is a Fermat liar for
+    every 2^(2^k) + 1) through the batch PRP path; each probable prime is then
+    proven prime by the deterministic test."""
+    bases = [b for b in range(8, 1000, 2) if b & (b - 1)]
+    res = gf.quick_batch(bases, 10)
+    assert all(r.gl_ok for r in res)
+    prp = [r.b for r in res if r.is_prp]
+    assert 824 in prp
+    for b in prp:
+        assert pm.prime(Transform(b, 10), b, 10).is_prime is True, b
+
+
+def test_prime_resumes_from_context(tmp_path):
+    ctx = str(tmp_path / "p.ctx")
+    r = pm.prime(Transform(150, 11), 150, 11, ctx=ctx, save_every=2000, abort_at=(1, 7000))
+    assert r.is_prime is None
+    r = pm.prime(Transform(150, 11), 150, 11, ctx=ctx)
+    assert r.is_prime is True

@@ -170,3 +170,57 @@ def test_tampered_proof_is_caught(oracle, tmp_path):
     with pytest.raises(pf.FileError):
         pf.server(oracle.OracleTransform(b, n, 4), b, n, str(tmp_path / "bad.proof"), str(tmp_path / "b.cert"),
                   (5, 20, 7))
+
+
+# ------------------------------------------------------------------ deterministic test (mode "prime")
+
+from genefer22_b200 import prime as pm
+
+
+def _jacobi(a: int, n: int) -> int:
+    """Textbook Jacobi symbol for odd n > 0, to check kronecker()."""
+    a %= n
+    r = 1
+    while a:
+        while a % 2 == 0:
+            a //= 2
+            if n % 8 in (3, 5):
+                r = -r
+        a, n = n, a
+        if a % 4 == 3 and n % 4 == 3:
+            r = -r
+        a %= n
+    return r if n == 1 else 0
+
+
+def test_kronecker_matches_jacobi():
+    for y in range(1, 400, 2):
+        for x in range(0, 200):
+            assert pm.kronecker(x, y) == _jacobi(x, y), (x, y)
+    assert pm.kronecker(2, 4) == 0
+
+
+def test_powmod_as_written():
+    # arith.h:13-25 multiplies once more by the last square: a^(2^(k+1)) for e = 2^k
+    for m in (7, 11, 101):
+        for a in range(2, 20):
+            for k in range(0, 6):
+                assert pm.powmod(a, 1 << k, m) == pow(a, 1 << (k + 1), m)
+
+
+def test_prime_factors_and_bases():
+    assert pm.prime_factors(824) == [2, 103]
+    assert pm.prime_factors(2 * 3 * 3 * 5 * 7 * 7 * 101) == [2, 3, 5, 7, 101]
+    it = pm.bases(824, 10)
+    got = [next(it)[1] for _ in range(6)]
+    a2 = pm.first_base(824, 10)
+    assert got[0] == a2 and 4 not in got and 9 not in got and got.count(a2) == 1
+
+
+def test_prime_on_oracle(oracle):
+    """824^(2^10)+1 is prime (the smallest even base at n = 10); 826^(2^10)+1
+    is composite; both decided through squareMul on the oracle engine."""
+    r = pm.prime(oracle.OracleTransform(824, 10), 824, 10)
+    assert r.is_prime is True and all(r.cond)
+    r = pm.prime(oracle.OracleTransform(826, 10), 826, 10)
+    assert r.is_prime is False
