@@ -186,10 +186,19 @@ struct Sched
 // one lane, all planes.  PM_FWD / PM_INV: r forward / inverse stages;
 // PM_MID_SQ / PM_MID_MUL: r forward stages, pointwise square (or product with
 // the multiplicand at zrow[PL * zstride + (lane << l) + i]), r inverse stages.
-template <int SET, int r, int MODE, int L, int SIGMA, class Map>
+//
+// IO selects where the group's elements come from and go to: IO_SMEM both in
+// the tile; IO_GIN loads from global memory (gmem + pl gstride + (lane << L) + i,
+// natural order) and stores to the tile; IO_GOUT loads from the tile and
+// stores to global memory.  The first forward and the last inverse pass of a
+// row read and write the planes in global memory directly (a warp takes 32
+// consecutive groups, so each of its 2^r accesses is one coalesced line).
+enum : int { IO_SMEM = 0, IO_GIN = 1, IO_GOUT = 2 };
+
+template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO = IO_SMEM>
 __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										 uint32_t base_step, const Tables &tab, const uint32_t *__restrict__ zrow,
-										 size_t zstride)
+										 size_t zstride, uint32_t *gmem = nullptr, size_t gstride = 0)
 {
 	constexpr int W = PrimeSet<SET>::W;
 	constexpr int E = 1 << r;
@@ -209,9 +218,19 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 		{
 			const auto z = prime_rt<SET>(pl);
 			uint32_t *pb = buf + pl * pstride + base;
+			uint32_t *gb = gmem;
+			if constexpr (IO != IO_SMEM) gb = gmem + pl * gstride + (static_cast<size_t>(lane) << L) + G.i0;
 			uint32_t x[E];
+			if constexpr (IO == IO_GIN)
+			{
 #pragma unroll
-			for (int m = 0; m < E; ++m) x[m] = pb[Map::off(m, STEP)];
+				for (int m = 0; m < E; ++m) x[m] = gb[m * STEP];
+			}
+			else
+			{
+#pragma unroll
+				for (int m = 0; m < E; ++m) x[m] = pb[Map::off(m, STEP)];
+			}
 			if constexpr (MODE != PM_INV) fwd_reg<decltype(z), r>(z, x, tb, tab.fw[pl]);
 			if constexpr (MODE == PM_MID_SQ)
 			{
@@ -226,8 +245,16 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 			}
 			if constexpr (MODE != PM_FWD)
 				inv_reg<decltype(z), r>(z, x, tb, tab.iv[pl], tb == 1u, __ldg(&tab.fw[pl][0]), __ldg(&tab.iv[pl][0]));
+			if constexpr (IO == IO_GOUT)
+			{
 #pragma unroll
-			for (int m = 0; m < E; ++m) pb[Map::off(m, STEP)] = x[m];
+				for (int m = 0; m < E; ++m) gb[m * STEP] = x[m];
+			}
+			else
+			{
+#pragma unroll
+				for (int m = 0; m < E; ++m) pb[Map::off(m, STEP)] = x[m];
+			}
 		}
 	}
 }
@@ -257,6 +284,44 @@ __device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_lo
 		pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
 															  nullptr, 0);
 		__syncthreads();
+	});
+}
+
+// Row transform of one row whose planes stay in global memory at g (plane
+// stride gstride): the first forward pass reads them, the last inverse pass
+// writes them, the passes between go through the shared-memory tile.
+// Squaring or product only (not OP_FWD).
+template <int SET, int L, class Map>
+__device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint32_t base0, const Tables &tab,
+												const uint32_t *zrow, size_t zstride, int op, uint32_t *g, size_t gstride)
+{
+	constexpr int NP = Sched<L>::NP;
+	static_assert(NP >= 2, "rows of at least two passes");
+	static_for<0, NP - 1>([&](auto P) {
+		constexpr int p = decltype(P)::value;
+		if constexpr (p == 0)
+			pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map, IO_GIN>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
+																		  g, gstride);
+		else
+			pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0);
+		__syncthreads();
+	});
+	constexpr int PL = NP - 1;
+	if (op == OP_MUL)
+		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride);
+	else
+		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride);
+	__syncthreads();
+	static_for<0, NP - 1>([&](auto Q) {
+		constexpr int p = NP - 2 - decltype(Q)::value;
+		if constexpr (p == 0)
+			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_GOUT>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
+																		   g, gstride);
+		else
+		{
+			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0);
+			__syncthreads();
+		}
 	});
 }
 
@@ -677,6 +742,12 @@ __device__ __forceinline__ void row_body(const Args &a, const TestDesc &d, uint3
 	uint32_t *buf = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(k) * S::C;
 	using MP = RowMap<LC>;
 
+	if (a.op != OP_FWD)
+	{
+		row_core_global<SET, LC, MP>(sm, S::PC, (1u << lr) + static_cast<uint32_t>(k), a.tab[SET],
+									 d.zp + static_cast<size_t>(k) * S::C, N, a.op, buf, N);
+		return;
+	}
 #pragma unroll
 	for (int pl = 0; pl < W; ++pl)
 		for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
