@@ -1,0 +1,37 @@
+"""A small, fixed squaring case for kernel profiles: one batch of `count`
+tests of size n (bases seeded uniform in [10^6, bmax), even), `squarings`
+squarings of register 0 with the given plan.
+
+    python -m genefer22_b200.profile_case --n 22 --count 1 --squarings 2
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+from .transform import Batch
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, required=True)
+    ap.add_argument("--count", type=int, default=1)
+    ap.add_argument("--bmax", type=int, default=35_000_000)
+    ap.add_argument("--plan", type=int, default=-1, help="-1: the default plan")
+    ap.add_argument("--squarings", type=int, default=2)
+    ap.add_argument("--seed", type=int, default=1)
+    a = ap.parse_args()
+    rng = np.random.default_rng(a.seed)
+    bases = [int(x) & ~1 for x in rng.integers(1_000_000, a.bmax, size=a.count)]
+    with Batch(bases, a.n) as bt:
+        if a.plan >= 0:
+            bt.set_plan(a.plan)
+        bt.set(3)
+        bt.square(False, a.squarings)
+        bt.sync()
+        print(f"n={a.n} tests={a.count} plan={bt.plan()} widths={sorted(set(bt.widths().tolist()))} squarings={a.squarings}")
+
+
+if __name__ == "__main__":
+    main()
