@@ -2,8 +2,9 @@
 
 A plan is the split of the length-N transform: ``lr = 0`` keeps a whole test
 in one CTA's shared memory (n <= 14); ``lr = 1`` keeps it in the shared
-memory of a thread-block cluster of 2^(n-13) CTAs (15 <= n <= 17); ``lr >= 3``
-runs the four-step form,
+memory of a thread-block cluster of 2^(n-13) CTAs (15 <= n <= 17); ``100 +
+lr2`` splits the column transform into a 16-point register pass and a
+2^lr2-point middle pass (six-step); ``lr >= 3`` runs the four-step form,
 2^lr-point column transforms (radix-16 register groups, 2^lr-point tiles in
 shared memory or registers) then 2^(n - lr)-point row transforms, the row
 pass carrying the pointwise product.  The prime set (RNS width, 2 or 3
@@ -38,6 +39,7 @@ SMALL_MAX_LOGN = 14
 
 
 PLAN_CLUSTER = 1
+PLAN_SIX = 100
 
 
 def candidates(n: int) -> List[int]:
@@ -49,6 +51,10 @@ def candidates(n: int) -> List[int]:
         lc = n - lr
         if 8 <= lc <= 13:
             out.append(lr)
+    for lr2 in range(3, 8):                 # six-step: 2^4 x 2^lr2 column split
+        lc = n - 4 - lr2
+        if 8 <= lc <= 13 and max(32, 4096 >> lr2) <= (1 << lc):
+            out.append(PLAN_SIX + lr2)
     return out
 
 

@@ -336,20 +336,57 @@ void launch_cluster_lq(int lq, const Args &a, int ntests, int max_active, cudaSt
 	}
 }
 
+// Six-step middle pass (k_mid): planes of every test, tiles of 2^lr2 rows.
+template <int LR2>
+void mid_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	using S = ColShape<LR2>;
+	if (prep) { set_smem(k_mid<LR2, false>, S::SMEM); set_smem(k_mid<LR2, true>, S::SMEM); return; }
+	const size_t C = size_t(1) << (a.n - MID_LR1 - LR2);
+	const dim3 grid(static_cast<unsigned>((size_t(1) << MID_LR1) * (C / S::CW)), static_cast<unsigned>(grid_y));
+	if (inv) k_mid<LR2, true><<<grid, col_threads(LR2), S::SMEM, s>>>(a);
+	else k_mid<LR2, false><<<grid, col_threads(LR2), S::SMEM, s>>>(a);
+	after_launch();
+}
+
+void launch_mid(int lr2, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	switch (lr2)
+	{
+		case 3: mid_t<3>(inv, a, grid_y, s, prep); break;
+		case 4: mid_t<4>(inv, a, grid_y, s, prep); break;
+		case 5: mid_t<5>(inv, a, grid_y, s, prep); break;
+		case 6: mid_t<6>(inv, a, grid_y, s, prep); break;
+		case 7: mid_t<7>(inv, a, grid_y, s, prep); break;
+		default: fail(GFC_ERR_ARG, "six-step plan needs 3 <= lr2 <= 7");
+	}
+}
+
+constexpr int PLAN_SIX = 100;     // plan codes 100 + lr2: six-step, 2^4 x 2^lr2 column split
+
 constexpr int PLAN_CLUSTER = 1;   // plan code of the cluster-resident squaring
 
 bool plan_valid(int n, int lr)
 {
 	if (lr == PLAN_CLUSTER) return (n >= 13 + 2) && (n <= 13 + 4);
+	if (lr > PLAN_SIX)
+	{
+		const int lr2 = lr - PLAN_SIX, lc = n - MID_LR1 - lr2;
+		return (lr2 >= 3) && (lr2 <= 7) && (lc >= 8) && (lc <= 13) && (col_width(lr2) <= (1 << lc));
+	}
 	if (lr == 0) return (n >= 10) && (n <= SMALL_MAX_LOGN);
 	const int lc = n - lr;
 	return (lr >= 3) && (lr <= 10) && (lc >= 8) && (lc <= 13) && ((lr <= 4) || (col_width(lr) <= (1 << lc)));
 }
 
+// Default plan code: single-CTA up to n = 14, four-step with rows of 2^12
+// (fewer below n = 15), six-step with rows of 2^12 from n = 21, where a
+// 2^(n-12)-point column tile would leave one or two CTAs per SM.
 int default_plan(int n)
 {
 	if (n <= SMALL_MAX_LOGN) return 0;
-	const int lc = (n >= 23) ? 13 : ((n - 3 < 12) ? n - 3 : 12);
+	if (n >= 21) return PLAN_SIX + (n - MID_LR1 - 12);
+	const int lc = (n - 3 < 12) ? n - 3 : 12;
 	return n - lc;
 }
 
@@ -382,6 +419,7 @@ struct gfc_batch
 	int pending = -1;             // register whose segment carries are not yet absorbed (four-step)
 	uint64_t sets_version = 0;    // bumped when a test changes prime set (per-set launches change)
 	int cluster = 0;              // log2 CTAs per cluster when squarings use k_cluster, else 0
+	int six = 0;                  // lr2 of a six-step plan (columns 2^4 x 2^lr2, lr = 4 + lr2), else 0
 	int cluster_max = 0;          // clusters of k_cluster resident at once
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
@@ -414,6 +452,25 @@ struct gfc_graph
 };
 
 namespace {
+
+// Sets the batch's kernels from a plan code (see gfc_batch_set_plan).
+void apply_plan(gfc_batch &bt, int code)
+{
+	bt.cluster = 0;
+	bt.six = 0;
+	if (code == PLAN_CLUSTER)
+	{
+		// products keep the default four-step plan of 15 <= n <= 17
+		bt.cluster = bt.n - ClusterShape<2>::LC;
+		bt.lr = default_plan(bt.n);
+	}
+	else if (code > PLAN_SIX)
+	{
+		bt.six = code - PLAN_SIX;
+		bt.lr = MID_LR1 + bt.six;
+	}
+	else bt.lr = code;
+}
 
 void check_reg(const gfc_batch &bt, size_t r)
 {
@@ -472,7 +529,8 @@ void prepare_plan(gfc_batch &bt)
 	if (bt.lr == 0) launch_small(bt, a, nullptr, true);
 	else
 	{
-		launch_col(bt.lr, false, a, 0, nullptr, true);
+		launch_col(bt.six ? MID_LR1 : bt.lr, false, a, 0, nullptr, true);
+		if (bt.six) launch_mid(bt.six, false, a, 0, nullptr, true);
 		launch_row(bt.n - bt.lr, a, 0, nullptr, true);
 	}
 }
@@ -483,6 +541,22 @@ void launch_fixup(gfc_batch &bt, const Args &a, int g)
 	const dim3 grid((nseg + FIX_THREADS - 1) / FIX_THREADS, static_cast<unsigned>(g));
 	k_fixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
 	after_launch();
+}
+
+// Column passes of the four-step (one kernel) or six-step (2^4-row column
+// kernel, then the middle pass; the reverse on the inverse side).
+void launch_cols_fwd(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
+{
+	if (bt.six == 0) { launch_col(bt.lr, false, a, g, s, false); return; }
+	launch_col(MID_LR1, false, a, g, s, false);
+	launch_mid(bt.six, false, a, g, s, false);
+}
+
+void launch_cols_inv(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
+{
+	if (bt.six == 0) { launch_col(bt.lr, true, a, g, s, false); return; }
+	launch_mid(bt.six, true, a, g, s, false);
+	launch_col(MID_LR1, true, a, g, s, false);
 }
 
 // Absorbs the pending segment carries of register bt.pending (k_fixup).
@@ -504,11 +578,11 @@ void fourstep(gfc_batch &bt, Args a)
 {
 	const int g = static_cast<int>(bt.count);
 	a.fix = (bt.pending >= 0 && bt.pending == a.src) ? 1 : 0;
-	launch_col(bt.lr, false, a, g, bt.stream, false);
+	launch_cols_fwd(bt, a, g, bt.stream);
 	if (a.fix) bt.pending = -1;
 	launch_row(bt.n - bt.lr, a, g, bt.stream, false);
 	if (a.op == OP_FWD) return;
-	launch_col(bt.lr, true, a, g, bt.stream, false);
+	launch_cols_inv(bt, a, g, bt.stream);
 	bt.pending = a.dst;
 }
 
@@ -625,11 +699,11 @@ void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
 			else
 			{
 				a.fix = (bt.pending == 0) ? 1 : 0;
-				launch_col(bt.lr, false, a, g, bt.stream, false);
+				launch_cols_fwd(bt, a, g, bt.stream);
 				GFC_CK(cudaEventRecord(ev[1], bt.stream));
 				launch_row(bt.n - bt.lr, a, g, bt.stream, false);
 				GFC_CK(cudaEventRecord(ev[2], bt.stream));
-				launch_col(bt.lr, true, a, g, bt.stream, false);
+				launch_cols_inv(bt, a, g, bt.stream);
 				bt.pending = 0;
 				GFC_CK(cudaEventRecord(ev[3], bt.stream));
 				GFC_CK(cudaEventSynchronize(ev[3]));
@@ -723,7 +797,7 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 		bt->nset[s]++;
 	}
 	bt->offset[0] = 0; bt->offset[1] = bt->nset[0];
-	bt->lr = default_plan(bt->n);
+	apply_plan(*bt, default_plan(bt->n));
 
 	GFC_CK(cudaSetDevice(device));
 	if (stream != nullptr) bt->stream = static_cast<cudaStream_t>(stream);
@@ -1119,24 +1193,16 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 		cudaSetDevice(bt->device);
 		materialize(*bt);
 		GFC_CK(cudaStreamSynchronize(bt->stream));
-		if (lr == PLAN_CLUSTER)
-		{
-			// products keep the default four-step plan
-			bt->cluster = bt->n - ClusterShape<2>::LC;
-			bt->lr = default_plan(bt->n);
-		}
-		else
-		{
-			bt->cluster = 0;
-			bt->lr = lr;
-		}
+		apply_plan(*bt, lr);
 		prepare_plan(*bt);
 	});
 }
 
 GFC_API int gfc_batch_plan(const gfc_batch *bt)
 {
-	return (bt == nullptr) ? GFC_ERR_ARG : ((bt->cluster > 0) ? PLAN_CLUSTER : bt->lr);
+	if (bt == nullptr) return GFC_ERR_ARG;
+	if (bt->cluster > 0) return PLAN_CLUSTER;
+	return (bt->six > 0) ? PLAN_SIX + bt->six : bt->lr;
 }
 
 GFC_API int gfc_batch_widths(const gfc_batch *bt, int32_t *w)

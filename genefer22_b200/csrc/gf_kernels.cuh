@@ -854,6 +854,69 @@ __global__ void __launch_bounds__(col_threads(LR)) k_col_inv(const Args a)
 	if (d.set == 0) col_inv_body<0, LR>(a, d, dup, sm); else col_inv_body<1, LR>(a, d, dup, sm);
 }
 
+// ---- six-step middle pass.
+//
+// With R = R1 R2 rows (R1 = 2^MID_LR1), the column transform of length R is
+// split: the R1-point column pass (stages 0 .. MID_LR1-1) is the four-step
+// column kernel of R1 rows over the same N, and this pass runs stages
+// MID_LR1 .. MID_LR1 + LR2 - 1: for block m < R1, rows m R2 .. m R2 + R2 - 1
+// of the R x C matrix hold 2^LR2-point transforms down each column with base
+// R1 + m.  Tile: R2 rows x CW columns of every plane, planes in and out.
+constexpr int MID_LR1 = 4;
+
+template <int SET, int LR2, bool INV>
+__device__ __forceinline__ void mid_body(const Args &a, const TestDesc &d, uint32_t *sm)
+{
+	using S = ColShape<LR2>;
+	constexpr int W = PrimeSet<SET>::W;
+	const int lr = MID_LR1 + LR2, lc = a.n - lr;
+	const size_t N = size_t(1) << a.n, C = size_t(1) << lc;
+	const int tiles = static_cast<int>(C / S::CW);
+	const int m = blockIdx.x / tiles;                      // block of R2 rows
+	const size_t c0 = static_cast<size_t>(blockIdx.x % tiles) * S::CW;
+	const size_t row0 = static_cast<size_t>(m) << LR2;
+	// the forward transform of a multiplicand (OP_FWD) lives in zp
+	uint32_t *planes = ((a.op == OP_FWD) ? d.zp : d.planes) + row0 * C + c0;
+	using MP = ColMap<S::RS>;
+	for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
+	{
+		const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
+#pragma unroll
+		for (int pl = 0; pl < W; ++pl)
+		{
+			const uint4 u = *reinterpret_cast<const uint4 *>(planes + pl * N + static_cast<size_t>(k) * C + cc);
+			uint32_t *p = sm + pl * S::PS + MP::addr(k, cc);
+			p[0] = u.x; p[1] = u.y; p[2] = u.z; p[3] = u.w;
+		}
+	}
+	__syncthreads();
+	const uint32_t base = (1u << MID_LR1) + static_cast<uint32_t>(m);
+	if constexpr (INV) run_inv<SET, LR2, false, MP>(sm, S::PS, S::CWL, true, base, 0u, a.tab[SET]);
+	else run_fwd<SET, LR2, false, MP>(sm, S::PS, S::CWL, true, base, 0u, a.tab[SET]);
+	for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
+	{
+		const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
+#pragma unroll
+		for (int pl = 0; pl < W; ++pl)
+		{
+			const uint32_t *p = sm + pl * S::PS + MP::addr(k, cc);
+			*reinterpret_cast<uint4 *>(planes + pl * N + static_cast<size_t>(k) * C + cc) = make_uint4(p[0], p[1], p[2], p[3]);
+		}
+	}
+}
+
+template <int LR2, bool INV>
+__global__ void __launch_bounds__(col_threads(LR2)) k_mid(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) mid_body<0, LR2, INV>(a, d, sm); else mid_body<1, LR2, INV>(a, d, sm);
+}
+
 // ---- four-step with R <= 16 rows: one thread owns a whole column.
 
 constexpr int COLR_THREADS = 256;

@@ -166,8 +166,10 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
 /* Kernel plan.  lr = 0: one CTA per test with the state in shared memory
  * (n <= 14); lr = 1: squarings by one thread-block cluster per test with the
  * state in the cluster's shared memory (15 <= n <= 17; products use the
- * default four-step plan); lr >= 3: four-step with R = 2^lr rows
- * (lr <= 10, 8 <= n - lr <= 13).  gfc_batch_plan reads the current plan. */
+ * default four-step plan); 3 <= lr <= 10: four-step with R = 2^lr rows
+ * (8 <= n - lr <= 13); lr = 100 + lr2 (3 <= lr2 <= 7): six-step, the column
+ * transform split into 2^4 and 2^lr2 points (8 <= n - 4 - lr2 <= 13).
+ * gfc_batch_plan reads the current plan. */
 int gfc_batch_set_plan(gfc_batch *bt, int lr);
 int gfc_batch_plan(const gfc_batch *bt);
 

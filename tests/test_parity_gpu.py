@@ -63,6 +63,13 @@ def test_four_step_plan(oracle, n, lr, b):
     check_ops(oracle, b, n, plan=lr, seed=100 + n + lr, steps=3)
 
 
+# six-step plans 100 + lr2: a 16-point column pass, a 2^lr2-point middle pass, rows
+@pytest.mark.parametrize("n,plan", [(16, 103), (16, 104), (17, 104), (18, 105), (19, 106), (20, 107), (21, 105)])
+@pytest.mark.parametrize("b", [SMALL_B, LARGE_B])
+def test_six_step_plan(oracle, n, plan, b):
+    check_ops(oracle, b, n, plan=plan, seed=200 + n + plan, steps=3)
+
+
 def test_width_choice():
     # 2 primes while N (b/2+1)^2 < P1 P2 / 2, else 3
     assert Transform(SMALL_B, 12).width() == 2
