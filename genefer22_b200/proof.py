@@ -32,7 +32,7 @@ import struct
 import time
 import zlib
 from dataclasses import dataclass
-from typing import Callable, Optional, Tuple
+from typing import Optional, Tuple
 
 import numpy as np
 

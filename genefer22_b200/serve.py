@@ -174,7 +174,7 @@ class _Pool:
         bt.set_exponent(slot, words, nb_pad)
         act.blocks_left = nb_pad // B
 
-    def _retire(self, slot: int, act: _Active, now: float):
+    def _retire(self, slot: int, act: _Active):
         bt = self.batch
         x = bt.get(slot, 0)
         d = bt.get(slot, 1)
@@ -214,7 +214,7 @@ class _Pool:
                         continue
                     act.blocks_left -= 1
                     if act.blocks_left == 0:
-                        self._retire(slot, act, srv.clock())
+                        self._retire(slot, act)
                 idle_since = srv.clock()
         except BaseException as e:            # surfaced by Server.run
             with srv.cv:

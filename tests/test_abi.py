@@ -1,7 +1,6 @@
 """CPU tests of the product's host side: the C ABI loads and exports every
 declared symbol, and the host-only functions (gint, exponent, schedule)
 agree with the oracle.  No GPU work is launched here."""
-import ctypes
 import os
 import re
 

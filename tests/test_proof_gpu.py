@@ -2,7 +2,6 @@
 keys consistent across the three modes, files byte-identical to the ones the
 oracle engine writes, and a run stopped and resumed from its context file
 ending where an uninterrupted run ends."""
-import numpy as np
 import pytest
 
 from genefer22_b200 import Transform

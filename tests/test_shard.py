@@ -4,7 +4,6 @@ standing in for a GPU)."""
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 from genefer22_b200.shard import predicted_cost, run_sharded, shard_tests
