@@ -4,13 +4,16 @@ A plan is the split of the length-N transform: ``lr = 0`` keeps a whole test
 in one CTA's shared memory (n <= 14); ``lr = 1`` keeps it in the shared
 memory of a thread-block cluster of 2^(n-13) CTAs (15 <= n <= 17); ``100 +
 lr2`` splits the column transform into a 16-point register pass and a
-2^lr2-point middle pass (six-step); ``lr >= 3`` runs the four-step form,
+2^lr2-point middle pass (six-step); ``200 + lr`` packs two base-b digits into
+one coefficient of a half-length transform over four primes (valid when every
+base of the batch lies in the exact range; the engine refuses it otherwise);
+``lr >= 3`` runs the four-step form,
 2^lr-point column transforms (radix-16 register groups, 2^lr-point tiles in
 shared memory or registers) then 2^(n - lr)-point row transforms, the row
-pass carrying the pointwise product.  The prime set (RNS width, 2 or 3
-primes) is not a free choice: the narrowest set whose product bounds the
-convolution exactly is always the fastest (one plane less of every pass), so
-the engine takes it per test and the tuner reports it.
+pass carrying the pointwise product.  Without packing, the prime set (2 or
+3 primes) follows from each base: the narrowest exact set is the fastest.
+The RNS width the tuner does choose is packing: four primes on half as many
+points instead of two or three on all of them.
 
 The reference has no counterpart: genefer runs one test per transform with a
 fixed GPU kernel split chosen from n (src/transformGPU.h:945-1083).
@@ -40,6 +43,7 @@ SMALL_MAX_LOGN = 14
 
 PLAN_CLUSTER = 1
 PLAN_SIX = 100
+PLAN_PACKED = 200
 
 
 def candidates(n: int) -> List[int]:
@@ -51,6 +55,9 @@ def candidates(n: int) -> List[int]:
         lc = n - lr
         if 8 <= lc <= 13:
             out.append(lr)
+    for lr in (3, 4):                       # packed digits: four primes, transform of N/2
+        if 8 <= n - 1 - lr <= 13:
+            out.append(PLAN_PACKED + lr)
     for lr2 in range(3, 8):                 # six-step: 2^4 x 2^lr2 column split
         lc = n - 4 - lr2
         if 8 <= lc <= 13 and max(32, 4096 >> lr2) <= (1 << lc):

@@ -52,14 +52,25 @@ template <> struct PrimeSet<0>
 {
 	static constexpr int W = 2;
 	static constexpr bool P31 = false;
-	static constexpr uint32_t p[3] = { 125u * (1u << 25) + 1u, 243u * (1u << 24) + 1u, 0u };
+	static constexpr uint32_t p[4] = { 125u * (1u << 25) + 1u, 243u * (1u << 24) + 1u, 0u, 0u };
 };
 
 template <> struct PrimeSet<1>
 {
 	static constexpr int W = 3;
 	static constexpr bool P31 = true;
-	static constexpr uint32_t p[3] = { 127u * (1u << 24) + 1u, 63u * (1u << 25) + 1u, 15u * (1u << 27) + 1u };
+	static constexpr uint32_t p[4] = { 127u * (1u << 24) + 1u, 63u * (1u << 25) + 1u, 15u * (1u << 27) + 1u, 0u };
+};
+
+// Set 2: four primes below 2^31 for packed digits (two base-b digits per
+// coefficient of a transform of N/2 points); the fourth, 249 * 2^23 + 1, has
+// 2^23 | p - 1, enough for N/2 <= 2^22.
+template <> struct PrimeSet<2>
+{
+	static constexpr int W = 4;
+	static constexpr bool P31 = true;
+	static constexpr uint32_t p[4] = { 127u * (1u << 24) + 1u, 63u * (1u << 25) + 1u, 249u * (1u << 23) + 1u,
+									   15u * (1u << 27) + 1u };
 };
 
 // ---------------------------------------------------------------- Zp (one prime)
@@ -143,10 +154,11 @@ struct ZpR
 template <int SET>
 __device__ __forceinline__ ZpR<PrimeSet<SET>::P31> prime_rt(int pl)
 {
-	constexpr uint32_t p0 = PrimeSet<SET>::p[0], p1 = PrimeSet<SET>::p[1], p2 = PrimeSet<SET>::p[2];
+	constexpr uint32_t p0 = PrimeSet<SET>::p[0], p1 = PrimeSet<SET>::p[1], p2 = PrimeSet<SET>::p[2],
+					   p3 = PrimeSet<SET>::p[3];
 	ZpR<PrimeSet<SET>::P31> z;
-	z.p = (pl == 0) ? p0 : ((pl == 1) ? p1 : p2);
-	z.q = (pl == 0) ? mont_qinv(p0) : ((pl == 1) ? mont_qinv(p1) : mont_qinv(p2));
+	z.p = (pl == 0) ? p0 : ((pl == 1) ? p1 : ((pl == 2) ? p2 : p3));
+	z.q = (pl == 0) ? mont_qinv(p0) : ((pl == 1) ? mont_qinv(p1) : ((pl == 2) ? mont_qinv(p2) : mont_qinv(p3)));
 	return z;
 }
 
@@ -171,6 +183,19 @@ struct Crt<1>
 	static constexpr uint32_t c12 = to_mont_c(invmod_c(p1 % p2, p2), p2);                                   // p1^{-1} mod p2
 	static constexpr uint32_t p1m3 = to_mont_c(p1 % p3, p3);                                                 // p1 mod p3
 	static constexpr uint32_t c123 = to_mont_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);   // (p1 p2)^{-1} mod p3
+};
+
+template <>
+struct Crt<2>
+{
+	static constexpr uint32_t p1 = PrimeSet<2>::p[0], p2 = PrimeSet<2>::p[1], p3 = PrimeSet<2>::p[2], p4 = PrimeSet<2>::p[3];
+	static constexpr uint32_t c12 = to_mont_c(invmod_c(p1 % p2, p2), p2);                                   // p1^{-1} mod p2
+	static constexpr uint32_t p1m3 = to_mont_c(p1 % p3, p3);
+	static constexpr uint32_t c123 = to_mont_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);
+	static constexpr uint32_t p1m4 = to_mont_c(p1 % p4, p4);
+	static constexpr uint32_t p12m4 = to_mont_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p4), p4);
+	static constexpr uint32_t c1234 = to_mont_c(invmod_c(static_cast<uint32_t>(
+		(((static_cast<uint64_t>(p1) * p2) % p4) * p3) % p4), p4), p4);                                 // (p1 p2 p3)^{-1} mod p4
 };
 
 // ---------------------------------------------------------------- CRT + base-b carry
@@ -264,6 +289,112 @@ __device__ __forceinline__ int32_t carry_small(int64_t s, const CarryK &K, int64
 	const uint64_t qv = divb64(static_cast<uint64_t>(s) + K.h + K.kb, K.b, K.binv, rv);
 	c = static_cast<int64_t>(qv - K.k);
 	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
+}
+
+// ---------------------------------------------------------------- packed digits (set 2)
+//
+// A coefficient of the packed transform is D = d0 + b d1 for two consecutive
+// balanced base-b digits.  After the inverse transform its CRT value is f V
+// (f = 1, or 2 for a doubled square), |V| < M/2 with M = p1 p2 p3 p4 < 2^124.
+// Garner gives V = a1 + p1 a2 + p1 p2 a3 + p1 p2 p3 a4 (a_k < p_k, minus M
+// when V > M/2).  Every weight w = f p1 ... p_{k-1} and f M is written in base
+// b on the host (limbs < b < 2^28), so that
+//     f V = sum_j U_j b^j,   U_j = sum_k a_k w_{k,j} - [V > M/2] (f M)_j,
+// a sum of products of 31- and 28-bit numbers.  The limbs shrink with j
+// (w1 < 2^33, w2 < 2^64, w3 < 2^95 and b >= 2^20 give |U_0|, |U_1| < 2^60.6,
+// |U_2| < 2^60, |U_3| < 2^59.1, |U_4| < 2^45, |U_5|, |U_6| < 2^28), and a
+// window position p collects U_{p-2i} of at most four coefficients i plus the
+// carry of the digit before it, so every position stays below 2^61.4 in
+// magnitude: the U_j are added to the window unsplit, two digits are completed
+// per coefficient (one 64-bit division each), and what remains after a
+// 16-digit segment (positions 16 .. 20) is the segment's carry, five values
+// below 2^62 added to the next segment's first five digits.
+
+constexpr int PK_LIMBS = 7;     // base-b limbs of f M (b >= 2^20, f M < 2^125)
+constexpr int PK_CARRY = 5;     // carry values per 16-digit segment
+
+// Per-test constants of the packed CRT + carry (host-computed); index f - 1.
+struct PackK
+{
+	uint32_t w1[2][2];          // limbs 0..1 of f p1
+	uint32_t w2[2][4];          // limbs 0..3 of f p1 p2
+	uint32_t w3[2][5];          // limbs 0..4 of f p1 p2 p3
+	uint32_t m[2][PK_LIMBS];    // limbs of f M
+	uint32_t bm[4];             // b mod p_k in Montgomery form (packing d0 + b d1)
+};
+
+// Adds the CRT value of one packed coefficient (residues x[4]) times f to the
+// window at positions 0..6.
+__device__ __forceinline__ void crt_window(const uint32_t x[4], int dup, const CarryK &K, const PackK &P, int64_t (&win)[7])
+{
+	using C = Crt<2>;
+	using Z2 = Zp<C::p2, true>;
+	using Z3 = Zp<C::p3, true>;
+	using Z4 = Zp<C::p4, true>;
+	const uint32_t a1 = x[0];
+	const uint32_t a1m2 = (a1 >= C::p2) ? a1 - C::p2 : a1;
+	const uint32_t a2 = Z2::mul(Z2::sub(x[1], a1m2), C::c12);
+	const uint32_t a1m3 = (a1 >= C::p3) ? a1 - C::p3 : a1;
+	const uint32_t a3 = Z3::mul(Z3::sub(x[2], Z3::add(a1m3, Z3::mul(a2, C::p1m3))), C::c123);
+	const uint32_t a1m4 = (a1 >= C::p4) ? a1 - C::p4 : a1;
+	const uint32_t a2m4 = (a2 >= C::p4) ? a2 - C::p4 : a2;
+	const uint32_t s4 = Z4::add(Z4::add(a1m4, Z4::mul(a2m4, C::p1m4)), Z4::mul(a3, C::p12m4));
+	const uint32_t a4 = Z4::mul(Z4::sub(x[3], s4), C::c1234);
+	// V > M/2 by mixed-radix digits from the top (M/2 = T (p4 - 1)/2 + T/2, T = p1 p2 p3)
+	constexpr uint64_t P12 = static_cast<uint64_t>(C::p1) * C::p2;
+	const uint64_t low = static_cast<uint64_t>(a2) * C::p1 + a1;            // < p1 p2
+	const bool rest_hi = (a3 > (C::p3 - 1) / 2) || ((a3 == (C::p3 - 1) / 2) && (low > P12 / 2));
+	const bool z = (a4 > (C::p4 - 1) / 2) || ((a4 == (C::p4 - 1) / 2) && rest_hi);
+	const int f = dup;                                                       // index f - 1
+	const int64_t zm = z ? 1 : 0;
+	const uint64_t A1 = a1, A2 = a2, A3 = a3, A4 = a4;
+	int64_t U[PK_LIMBS];
+	U[0] = static_cast<int64_t>((A1 << dup) + A2 * P.w1[f][0] + A3 * P.w2[f][0] + A4 * P.w3[f][0]) - zm * P.m[f][0];
+	U[1] = static_cast<int64_t>(A2 * P.w1[f][1] + A3 * P.w2[f][1] + A4 * P.w3[f][1]) - zm * P.m[f][1];
+	U[2] = static_cast<int64_t>(A3 * P.w2[f][2] + A4 * P.w3[f][2]) - zm * P.m[f][2];
+	U[3] = static_cast<int64_t>(A3 * P.w2[f][3] + A4 * P.w3[f][3]) - zm * P.m[f][3];
+	U[4] = static_cast<int64_t>(A4 * P.w3[f][4]) - zm * P.m[f][4];
+	U[5] = -zm * P.m[f][5];
+	U[6] = -zm * P.m[f][6];
+#pragma unroll
+	for (int j = 0; j < PK_LIMBS; ++j) win[j] += U[j];
+}
+
+// Completes the digit at window position 0 and shifts the window by one.
+__device__ __forceinline__ int32_t window_digit(const CarryK &K, int64_t (&win)[7])
+{
+	int64_t q;
+	const int32_t d = carry_wide(win[0], K, q);
+#pragma unroll
+	for (int j = 0; j < 6; ++j) win[j] = win[j + 1];
+	win[6] = 0;
+	win[0] += q;
+	return d;
+}
+
+// Adds a packed segment carry (c[k] at digit k, k < 5) to D consecutive
+// digits, reducing until the running carry is 0 or +-1, which stays in the
+// next digit unreduced (|digit| <= b/2 + 1); false if the carry did not fit.
+template <int D>
+__device__ __forceinline__ bool absorb5(int32_t (&dg)[D], const int64_t (&c)[PK_CARRY], const CarryK &K)
+{
+	int64_t q = 0;
+	bool done = false;
+#pragma unroll
+	for (int k = 0; k < D; ++k)
+	{
+		if (done) continue;
+		const int64_t in = (k < PK_CARRY) ? c[k] : 0;
+		if ((k >= PK_CARRY) && (q >= -1) && (q <= 1))
+		{
+			dg[k] += static_cast<int32_t>(q);
+			q = 0;
+			done = true;
+			continue;
+		}
+		dg[k] = carry_wide(static_cast<int64_t>(dg[k]) + in + q, K, q);
+	}
+	return done || (q == 0);
 }
 
 }  // namespace gfc

@@ -113,7 +113,7 @@ struct DeviceTables
 {
 	int device = -1, n = 0;
 	uint32_t *d = nullptr;
-	Tables tab[2];
+	Tables tab[3];
 	~DeviceTables()
 	{
 		if (d != nullptr) { cudaSetDevice(device); cudaFree(d); }
@@ -167,6 +167,69 @@ int choose_set(uint32_t b, int n)
 	if (bound < M0 / 2) return 0;
 	if (bound < M1 / 2) return 1;
 	return -1;
+}
+
+// Root tables of prime set 2 for the packed transform of 2^np points
+// (cached under key -np).
+std::shared_ptr<DeviceTables> get_tables_packed(int device, int np)
+{
+	std::lock_guard<std::mutex> lock(g_tab_mu);
+	const auto key = std::make_pair(device, -np);
+	auto it = g_tab_cache.find(key);
+	if (it != g_tab_cache.end())
+		if (auto sp = it->second.lock()) return sp;
+	auto t = std::make_shared<DeviceTables>();
+	t->device = device; t->n = np;
+	const size_t N = size_t(1) << np;
+	GFC_CK(cudaMalloc(&t->d, 8 * N * sizeof(uint32_t)));
+	std::vector<uint32_t> fw(N), iv(N);
+	for (int pl = 0; pl < 4; ++pl)
+	{
+		build_roots(PrimeSet<2>::p[pl], np, fw.data(), iv.data());
+		GFC_CK(cudaMemcpy(t->d + (2 * pl) * N, fw.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		GFC_CK(cudaMemcpy(t->d + (2 * pl + 1) * N, iv.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		t->tab[2].fw[pl] = t->d + (2 * pl) * N;
+		t->tab[2].iv[pl] = t->d + (2 * pl + 1) * N;
+	}
+	g_tab_cache[key] = t;
+	return t;
+}
+
+// Packed digits (two base-b digits per coefficient, prime set 2) are exact
+// when every coefficient of the half-length product, at most
+// (N/2) ((b/2 + 1)(b + 1))^2, is below floor(M_2 / 2); the limb split of the
+// CRT value wants 2^20 <= b < 2^28.
+bool packed_ok(uint32_t b, int n)
+{
+	if ((b < (1u << 20)) || (b >= (1u << 28))) return false;
+	const u128 D = u128(b / 2 + 1) * (u128(b) + 1);
+	const u128 M2 = u128(PrimeSet<2>::p[0]) * PrimeSet<2>::p[1] * PrimeSet<2>::p[2] * PrimeSet<2>::p[3];
+	return D * D < (M2 / 2) / (u128(1) << (n - 1));
+}
+
+void base_limbs(u128 w, uint32_t b, uint32_t *out, int count)
+{
+	for (int j = 0; j < count; ++j) { out[j] = static_cast<uint32_t>(w % b); w /= b; }
+	if (w != 0) fail(GFC_ERR_RANGE, "packed digits: weight does not fit its limbs");
+}
+
+PackK pack_constants(uint32_t b)
+{
+	PackK P{};
+	const u128 p1 = PrimeSet<2>::p[0], p2 = PrimeSet<2>::p[1], p3 = PrimeSet<2>::p[2], p4 = PrimeSet<2>::p[3];
+	for (int f = 1; f <= 2; ++f)
+	{
+		base_limbs(f * p1, b, P.w1[f - 1], 2);
+		base_limbs(f * p1 * p2, b, P.w2[f - 1], 4);
+		base_limbs(f * p1 * p2 * p3, b, P.w3[f - 1], 5);
+		base_limbs(f * p1 * p2 * p3 * p4, b, P.m[f - 1], PK_LIMBS);
+	}
+	for (int k = 0; k < 4; ++k)
+	{
+		const uint32_t p = PrimeSet<2>::p[k];
+		P.bm[k] = static_cast<uint32_t>((static_cast<uint64_t>(b % p) << 32) % p);
+	}
+	return P;
 }
 
 // Constants of the fused CRT + carry (gf_arith.cuh, CarryK) for base b.
@@ -267,27 +330,52 @@ void launch_col(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, boo
 	}
 }
 
+// Rows of 2^LC points; `planes` = 3, or 4 for packed digits (prime set 2),
+// sets the shared memory of the launch.
 template <int LC>
-void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep)
+void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 {
 	using S = RowShape<LC>;
-	if (prep) { set_smem(k_row<LC>, S::SMEM); return; }
+	const size_t smem = size_t(planes) * S::PC * 4;
+	if (prep) { set_smem(k_row<LC>, size_t(4) * S::PC * 4); return; }
 	const dim3 grid(1u << (a.n - LC), static_cast<unsigned>(grid_y));
-	k_row<LC><<<grid, row_threads(LC), S::SMEM, s>>>(a);
+	k_row<LC><<<grid, row_threads(LC), smem, s>>>(a);
 	after_launch();
 }
 
-void launch_row(int lc, const Args &a, int grid_y, cudaStream_t s, bool prep)
+void launch_row(int lc, const Args &a, int grid_y, cudaStream_t s, bool prep, int planes = 3)
 {
 	switch (lc)
 	{
-		case 8: row_t<8>(a, grid_y, s, prep); break;
-		case 9: row_t<9>(a, grid_y, s, prep); break;
-		case 10: row_t<10>(a, grid_y, s, prep); break;
-		case 11: row_t<11>(a, grid_y, s, prep); break;
-		case 12: row_t<12>(a, grid_y, s, prep); break;
-		case 13: row_t<13>(a, grid_y, s, prep); break;
+		case 8: row_t<8>(a, grid_y, s, prep, planes); break;
+		case 9: row_t<9>(a, grid_y, s, prep, planes); break;
+		case 10: row_t<10>(a, grid_y, s, prep, planes); break;
+		case 11: row_t<11>(a, grid_y, s, prep, planes); break;
+		case 12: row_t<12>(a, grid_y, s, prep, planes); break;
+		case 13: row_t<13>(a, grid_y, s, prep, planes); break;
 		default: fail(GFC_ERR_ARG, "four-step plan needs 8 <= n - lr <= 13");
+	}
+}
+
+// Packed column kernels (prime set 2), a.n = log2 of the packed length.
+template <int LR>
+void pcol_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	using S = PColShape<LR>;
+	if (prep) { set_smem(k_pcol_inv<LR>, S::SMEM); return; }
+	const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / PCOL_THREADS), static_cast<unsigned>(grid_y));
+	if (inv) k_pcol_inv<LR><<<grid, PCOL_THREADS, S::SMEM, s>>>(a);
+	else k_pcol_fwd<LR><<<grid, PCOL_THREADS, 0, s>>>(a);
+	after_launch();
+}
+
+void launch_pcol(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+{
+	switch (lr)
+	{
+		case 3: pcol_t<3>(inv, a, grid_y, s, prep); break;
+		case 4: pcol_t<4>(inv, a, grid_y, s, prep); break;
+		default: fail(GFC_ERR_ARG, "packed plan needs lr = 3 or 4");
 	}
 }
 
@@ -363,11 +451,17 @@ void launch_mid(int lr2, bool inv, const Args &a, int grid_y, cudaStream_t s, bo
 }
 
 constexpr int PLAN_SIX = 100;     // plan codes 100 + lr2: six-step, 2^4 x 2^lr2 column split
+constexpr int PLAN_PACKED = 200;  // plan codes 200 + lr: packed digits, four-step of n - 1 with lr = 3, 4
 
 constexpr int PLAN_CLUSTER = 1;   // plan code of the cluster-resident squaring
 
 bool plan_valid(int n, int lr)
 {
+	if (lr > PLAN_PACKED)
+	{
+		const int l = lr - PLAN_PACKED, lc = n - 1 - l;
+		return (l >= 3) && (l <= 4) && (lc >= 8) && (lc <= 13);
+	}
 	if (lr == PLAN_CLUSTER) return (n >= 13 + 2) && (n <= 13 + 4);
 	if (lr > PLAN_SIX)
 	{
@@ -420,6 +514,8 @@ struct gfc_batch
 	uint64_t sets_version = 0;    // bumped when a test changes prime set (per-set launches change)
 	int cluster = 0;              // log2 CTAs per cluster when squarings use k_cluster, else 0
 	int six = 0;                  // lr2 of a six-step plan (columns 2^4 x 2^lr2, lr = 4 + lr2), else 0
+	bool packed = false;          // prime set 2, two digits per coefficient, transform of N/2 (lr of that)
+	std::shared_ptr<DeviceTables> tabp;   // root tables of prime set 2 at length N/2
 	int cluster_max = 0;          // clusters of k_cluster resident at once
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
@@ -453,12 +549,41 @@ struct gfc_graph
 
 namespace {
 
+// Switches every test's descriptor between its own prime set (0 or 1, digits
+// one per coefficient) and prime set 2 (packed digits).
+void set_packed(gfc_batch &bt, bool on)
+{
+	for (size_t i = 0; i < bt.count; ++i)
+	{
+		TestDesc &d = bt.h_desc[i];
+		if (on)
+		{
+			d.set = 2;
+			d.ck = carry_constants(bt.b[i], 1);
+			d.pk = pack_constants(bt.b[i]);
+		}
+		else
+		{
+			d.set = bt.set[i];
+			d.ck = carry_constants(bt.b[i], bt.set[i]);
+		}
+	}
+	if (on) bt.tabp = get_tables_packed(bt.device, bt.n - 1);
+	GFC_CK(cudaMemcpy(bt.d_desc, bt.h_desc.data(), bt.count * sizeof(TestDesc), cudaMemcpyHostToDevice));
+}
+
 // Sets the batch's kernels from a plan code (see gfc_batch_set_plan).
 void apply_plan(gfc_batch &bt, int code)
 {
 	bt.cluster = 0;
 	bt.six = 0;
-	if (code == PLAN_CLUSTER)
+	bt.packed = false;
+	if (code > PLAN_PACKED)
+	{
+		bt.packed = true;
+		bt.lr = code - PLAN_PACKED;
+	}
+	else if (code == PLAN_CLUSTER)
 	{
 		// products keep the default four-step plan of 15 <= n <= 17
 		bt.cluster = bt.n - ClusterShape<2>::LC;
@@ -496,6 +621,7 @@ Args make_args(const gfc_batch &bt)
 	a.err = bt.d_err;
 	a.tab[0] = bt.tab->tab[0];
 	a.tab[1] = bt.tab->tab[1];
+	if (bt.tabp) a.tab[2] = bt.tabp->tab[2];
 	a.n = bt.n;
 	a.lr = bt.lr;
 	a.num_regs = static_cast<int>(bt.num_regs);
@@ -526,7 +652,12 @@ void prepare_plan(gfc_batch &bt)
 	Args a{};
 	a.n = bt.n;
 	if (bt.cluster > 0) launch_cluster_lq(bt.cluster, a, 0, 0, nullptr, true, &bt.cluster_max);
-	if (bt.lr == 0) launch_small(bt, a, nullptr, true);
+	if (bt.packed)
+	{
+		launch_pcol(bt.lr, true, a, 0, nullptr, true);
+		launch_row(bt.n - 1 - bt.lr, a, 0, nullptr, true);
+	}
+	else if (bt.lr == 0) launch_small(bt, a, nullptr, true);
 	else
 	{
 		launch_col(bt.six ? MID_LR1 : bt.lr, false, a, 0, nullptr, true);
@@ -539,14 +670,24 @@ void launch_fixup(gfc_batch &bt, const Args &a, int g)
 {
 	const unsigned nseg = static_cast<unsigned>(bt.N / SEG);
 	const dim3 grid((nseg + FIX_THREADS - 1) / FIX_THREADS, static_cast<unsigned>(g));
-	k_fixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
+	if (bt.packed) k_pfixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
+	else k_fixup<<<grid, FIX_THREADS, 0, bt.stream>>>(a);
 	after_launch();
 }
 
 // Column passes of the four-step (one kernel) or six-step (2^4-row column
 // kernel, then the middle pass; the reverse on the inverse side).
+// Packed plans run the same passes on the half-length transform (a.n = n - 1).
+Args packed_args(const gfc_batch &bt, const Args &a)
+{
+	Args p = a;
+	p.n = bt.n - 1;
+	return p;
+}
+
 void launch_cols_fwd(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
 {
+	if (bt.packed) { launch_pcol(bt.lr, false, packed_args(bt, a), g, s, false); return; }
 	if (bt.six == 0) { launch_col(bt.lr, false, a, g, s, false); return; }
 	launch_col(MID_LR1, false, a, g, s, false);
 	launch_mid(bt.six, false, a, g, s, false);
@@ -554,9 +695,16 @@ void launch_cols_fwd(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
 
 void launch_cols_inv(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
 {
+	if (bt.packed) { launch_pcol(bt.lr, true, packed_args(bt, a), g, s, false); return; }
 	if (bt.six == 0) { launch_col(bt.lr, true, a, g, s, false); return; }
 	launch_mid(bt.six, true, a, g, s, false);
 	launch_col(MID_LR1, true, a, g, s, false);
+}
+
+void launch_rows(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
+{
+	if (bt.packed) launch_row(bt.n - 1 - bt.lr, packed_args(bt, a), g, s, false, 4);
+	else launch_row(bt.n - bt.lr, a, g, s, false, 3);
 }
 
 // Absorbs the pending segment carries of register bt.pending (k_fixup).
@@ -580,7 +728,7 @@ void fourstep(gfc_batch &bt, Args a)
 	a.fix = (bt.pending >= 0 && bt.pending == a.src) ? 1 : 0;
 	launch_cols_fwd(bt, a, g, bt.stream);
 	if (a.fix) bt.pending = -1;
-	launch_row(bt.n - bt.lr, a, g, bt.stream, false);
+	launch_rows(bt, a, g, bt.stream);
 	if (a.op == OP_FWD) return;
 	launch_cols_inv(bt, a, g, bt.stream);
 	bt.pending = a.dst;
@@ -701,7 +849,7 @@ void time_kernels(gfc_batch &bt, uint32_t reps, float *ms)
 				a.fix = (bt.pending == 0) ? 1 : 0;
 				launch_cols_fwd(bt, a, g, bt.stream);
 				GFC_CK(cudaEventRecord(ev[1], bt.stream));
-				launch_row(bt.n - bt.lr, a, g, bt.stream, false);
+				launch_rows(bt, a, g, bt.stream);
 				GFC_CK(cudaEventRecord(ev[2], bt.stream));
 				launch_cols_inv(bt, a, g, bt.stream);
 				bt.pending = 0;
@@ -807,7 +955,7 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 	const size_t N = bt->N;
 	auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
 	const size_t s_regs = al(count * num_regs * N * 4), s_pl = al(count * 3 * N * 4), s_zp = s_pl;
-	const size_t s_car = al(count * (N / SEG) * 8), s_desc = al(count * sizeof(TestDesc)), s_tests = al(count * 4);
+	const size_t s_car = al(count * (N / SEG) * 8 * PK_CARRY), s_desc = al(count * sizeof(TestDesc)), s_tests = al(count * 4);
 	const size_t s_pos = al(count * 8), s_err = 256;
 	bt->mem_bytes = s_regs + s_pl + s_zp + s_car + s_desc + s_tests + s_pos + s_err;
 	GFC_CK(cudaMalloc(&bt->mem, bt->mem_bytes));
@@ -834,7 +982,7 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 		d.regs = bt->regs + i * num_regs * N;
 		d.planes = bt->planes + i * 3 * N;
 		d.zp = bt->zp + i * 3 * N;
-		d.carry = bt->carry + i * (N / SEG);
+		d.carry = bt->carry + i * (N / SEG) * PK_CARRY;
 		d.ebits = nullptr;
 		d.b = b[i];
 		d.set = bt->set[i];
@@ -1063,10 +1211,17 @@ GFC_API int gfc_batch_assign(gfc_batch *bt, size_t test, uint32_t b)
 		for (int k = 0; k < 2; ++k)
 			for (size_t i = 0; i < bt->count; ++i)
 				if (bt->set[i] == k) tests.push_back(static_cast<int32_t>(i));
+		if (bt->packed && !packed_ok(b, bt->n)) fail(GFC_ERR_RANGE, "assign: base outside the range of packed digits");
 		TestDesc &d = bt->h_desc[test];
 		d.b = b;
 		d.set = s;
 		d.ck = carry_constants(b, s);
+		if (bt->packed)
+		{
+			d.set = 2;
+			d.ck = carry_constants(b, 1);
+			d.pk = pack_constants(b);
+		}
 		GFC_CK(cudaMemcpy(bt->d_desc + test, &d, sizeof(TestDesc), cudaMemcpyHostToDevice));
 		GFC_CK(cudaMemcpy(bt->d_tests, tests.data(), bt->count * sizeof(int32_t), cudaMemcpyHostToDevice));
 		prepare_plan(*bt);
@@ -1189,10 +1344,15 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 	return guard([&] {
 		GFC_NULLCHK(bt);
 		if (!plan_valid(bt->n, lr)) fail(GFC_ERR_ARG, "set_plan: invalid plan for this n");
+		const bool packed = lr > PLAN_PACKED;
+		if (packed)
+			for (size_t i = 0; i < bt->count; ++i)
+				if (!packed_ok(bt->b[i], bt->n)) fail(GFC_ERR_RANGE, "set_plan: a base is outside the range of packed digits");
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
-		materialize(*bt);
+		materialize(*bt);                 // pending carries are in the current plan's format
 		GFC_CK(cudaStreamSynchronize(bt->stream));
+		if (packed != bt->packed) set_packed(*bt, packed);
 		apply_plan(*bt, lr);
 		prepare_plan(*bt);
 	});
@@ -1201,6 +1361,7 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 GFC_API int gfc_batch_plan(const gfc_batch *bt)
 {
 	if (bt == nullptr) return GFC_ERR_ARG;
+	if (bt->packed) return PLAN_PACKED + bt->lr;
 	if (bt->cluster > 0) return PLAN_CLUSTER;
 	return (bt->six > 0) ? PLAN_SIX + bt->six : bt->lr;
 }
@@ -1209,7 +1370,7 @@ GFC_API int gfc_batch_widths(const gfc_batch *bt, int32_t *w)
 {
 	return guard([&] {
 		GFC_NULLCHK(bt); GFC_NULLCHK(w);
-		for (size_t i = 0; i < bt->count; ++i) w[i] = (bt->set[i] == 0) ? 2 : 3;
+		for (size_t i = 0; i < bt->count; ++i) w[i] = bt->packed ? 4 : ((bt->set[i] == 0) ? 2 : 3);
 	});
 }
 
@@ -1294,9 +1455,9 @@ constexpr size_t NA_OFF_TAB = 0;                                  // 5 primes x 
 constexpr size_t NA_OFF_PLANES = NA_OFF_TAB + 10 * NA_N;          // 3 planes x N
 constexpr size_t NA_OFF_CARRY = NA_OFF_PLANES + 3 * NA_N;         // N/16 int64 carries
 constexpr size_t NA_OFF_DESC = NA_OFF_CARRY + NA_N / 8;           // one TestDesc
-constexpr size_t NA_OFF_MISC = NA_OFF_DESC + 64;                  // test index, position, error word
+constexpr size_t NA_OFF_MISC = NA_OFF_DESC + 128;                 // test index, position, error word
 constexpr size_t NA_WORDS = NA_OFF_MISC + 64;                     // 3.44 MB
-static_assert(sizeof(TestDesc) <= 64 * sizeof(uint32_t), "descriptor slot");
+static_assert(sizeof(TestDesc) <= 128 * sizeof(uint32_t), "descriptor slot");
 
 static __device__ __align__(256) uint32_t g_na_scratch[NA_WORDS];
 

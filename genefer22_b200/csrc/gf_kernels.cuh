@@ -41,14 +41,15 @@ struct TestDesc
 	int64_t *carry;         // N / SEG segment carries
 	const uint32_t *ebits;  // exponent bits, bit i in word i/32 (may be null)
 	CarryK ck;              // constants of the fused CRT + carry for this b
+	PackK pk;               // packed-digit constants (set 2)
 	uint32_t b;
-	int32_t set;            // prime set: 0 (W = 2), 1 (W = 3)
+	int32_t set;            // prime set: 0 (W = 2), 1 (W = 3), 2 (W = 4, packed digits)
 };
 
 struct Tables
 {
-	const uint32_t *fw[3];  // forward roots, Montgomery form; fw[p][0] = normalisation c
-	const uint32_t *iv[3];  // inverse roots, Montgomery form; iv[p][0] = K (last stage)
+	const uint32_t *fw[4];  // forward roots, Montgomery form; fw[p][0] = normalisation c
+	const uint32_t *iv[4];  // inverse roots, Montgomery form; iv[p][0] = K (last stage)
 };
 
 struct Args
@@ -57,7 +58,7 @@ struct Args
 	const int32_t *tests;   // indices of the tests this launch serves
 	int64_t *pos;           // per-test current exponent bit index
 	uint32_t *err;          // error flags (bit 0: carry not absorbed)
-	Tables tab[2];          // root tables of prime set 0 and 1
+	Tables tab[3];          // root tables of prime sets 0, 1 (length N) and 2 (length N/2)
 	int n, lr;              // log2 N, log2 R (four-step)
 	int num_regs, src, dst; // registers
 	int op, dup_mode, count, j;  // operation, dup source, squarings (k_small), squaring index in block
@@ -72,7 +73,8 @@ __device__ __forceinline__ void for_planes(F &&f)
 {
 	f(std::integral_constant<int, 0>{});
 	f(std::integral_constant<int, 1>{});
-	if constexpr (PrimeSet<SET>::W == 3) f(std::integral_constant<int, 2>{});
+	if constexpr (PrimeSet<SET>::W >= 3) f(std::integral_constant<int, 2>{});
+	if constexpr (PrimeSet<SET>::W >= 4) f(std::integral_constant<int, 3>{});
 }
 
 template <int B, int E, class F>
@@ -838,7 +840,9 @@ __global__ void __launch_bounds__(row_threads(LC)) k_row(const Args a)
 	bool active;
 	(void)get_dup(a, d, t, a.j, active);
 	if (!active) return;
-	if (d.set == 0) row_body<0, LC>(a, d, sm); else row_body<1, LC>(a, d, sm);
+	if (d.set == 0) row_body<0, LC>(a, d, sm);
+	else if (d.set == 1) row_body<1, LC>(a, d, sm);
+	else row_body<2, LC>(a, d, sm);
 }
 
 // Columns: last log2 R inverse stages, CRT, carry inside 16-digit segments.
@@ -1040,6 +1044,211 @@ __global__ void __launch_bounds__(COLR_THREADS) k_colr_inv(const Args a)
 	const bool dup = get_dup(a, d, t, a.j, active);
 	if (!active) return;
 	if (d.set == 0) col_inv_reg_body<0, LR>(a, d, dup, sm); else col_inv_reg_body<1, LR>(a, d, dup, sm);
+}
+
+// ---- packed digits (prime set 2).
+//
+// Coefficient i of the packed transform (N' = N/2 points, a.n = n - 1 in these
+// launches) is D_i = d_2i + b d_2i+1.  A 16-digit carry segment is 8
+// coefficients; its carry is PK_CARRY values (d.carry[PK_CARRY s + k]).
+// Register column kernels (R = 2^LR <= 16 rows, a thread per packed column);
+// the rows are k_row with prime set 2.
+
+constexpr int PCOL_THREADS = 256;
+
+// Takes (and clears) the packed carry into segment s: the previous
+// segment's, negated across the wrap (b^N = -1).
+__device__ __forceinline__ void take_carry5(const TestDesc &d, size_t s, size_t nseg, int64_t (&c)[PK_CARRY])
+{
+	const size_t src = (s == 0) ? nseg - 1 : s - 1;
+	int64_t *const p = d.carry + PK_CARRY * src;
+#pragma unroll
+	for (int k = 0; k < PK_CARRY; ++k)
+	{
+		const int64_t v = p[k];
+		if (v != 0) p[k] = 0;
+		c[k] = (s == 0) ? -v : v;
+	}
+}
+
+__device__ __forceinline__ void fix_segment5(const TestDesc &d, int32_t *seg, int32_t *g, size_t s, size_t nseg,
+											 uint32_t *err)
+{
+	int64_t c[PK_CARRY];
+	take_carry5(d, s, nseg, c);
+	bool any = false;
+#pragma unroll
+	for (int k = 0; k < PK_CARRY; ++k) any |= (c[k] != 0);
+	if (!any) return;
+	int32_t dg[SEG];
+#pragma unroll
+	for (int i = 0; i < SEG; ++i) dg[i] = seg[i];
+	if (!absorb5<SEG>(dg, c, d.ck)) atomicOr(err, 1u);
+#pragma unroll
+	for (int i = 0; i < SEG; ++i) { seg[i] = dg[i]; g[i] = dg[i]; }
+}
+
+// Digits -> packed residues -> first LR forward stages (one packed column per
+// thread); absorbs pending packed carries of register src first.
+template <int LR>
+__device__ __forceinline__ void pcol_fwd_body(const Args &a, const TestDesc &d, int32_t *sm)
+{
+	constexpr int R = 1 << LR, T = PCOL_THREADS, RW = 2 * T + 2;
+	const size_t Np = size_t(1) << a.n, Cp = size_t(1) << (a.n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x;
+	int32_t *const srcreg = d.regs + static_cast<size_t>(a.src) * (2 * Np);
+	uint32_t *dst = ((a.op == OP_FWD) ? d.zp : d.planes) + c0 + tid;
+	int32_t d0[R], d1[R];
+#pragma unroll
+	for (int k = 0; k < R; ++k)
+	{
+		const int2 v = *reinterpret_cast<const int2 *>(srcreg + 2 * (static_cast<size_t>(k) * Cp + c0 + tid));
+		d0[k] = v.x; d1[k] = v.y;
+	}
+	if (a.fix)
+	{
+#pragma unroll
+		for (int k = 0; k < R; ++k) { sm[k * RW + 2 * tid] = d0[k]; sm[k * RW + 2 * tid + 1] = d1[k]; }
+		__syncthreads();
+		const size_t nseg = (2 * Np) / SEG;
+		for (int e = tid; e < R * (2 * T / SEG); e += T)
+		{
+			const int k = e / (2 * T / SEG), s = e % (2 * T / SEG);
+			const size_t j0 = 2 * (static_cast<size_t>(k) * Cp + c0) + static_cast<size_t>(s) * SEG;
+			fix_segment5(d, sm + k * RW + s * SEG, srcreg + j0, j0 / SEG, nseg, a.err);
+		}
+		__syncthreads();
+#pragma unroll
+		for (int k = 0; k < R; ++k) { d0[k] = sm[k * RW + 2 * tid]; d1[k] = sm[k * RW + 2 * tid + 1]; }
+	}
+	for_planes<2>([&](auto PLc) {
+		constexpr int PL = decltype(PLc)::value;
+		using Z = ZS<2, PL>;
+		const uint32_t bm = d.pk.bm[PL];
+		uint32_t x[R];
+#pragma unroll
+		for (int k = 0; k < R; ++k) x[k] = Z::add(Z::from_int(d0[k]), Z::mul(Z::from_int(d1[k]), bm));
+		fwd_reg<Z, LR>(Z{}, x, 1u, a.tab[2].fw[PL]);
+#pragma unroll
+		for (int k = 0; k < R; ++k) dst[PL * Np + k * Cp] = x[k];
+	});
+}
+
+// Tile of the packed inverse column kernel: coefficient c of row k at
+// k RS + (c % 8) Q + c / 8 with Q = T/8 + 4, so that a warp writing 32
+// consecutive coefficients and a warp reading coefficient ci of 32
+// consecutive 8-coefficient segments both hit 32 distinct banks.
+template <int LR>
+struct PColShape
+{
+	static constexpr int R = 1 << LR, T = PCOL_THREADS, Q = T / 8 + 4, RS = 8 * Q, PS = R * RS;
+	static constexpr size_t SMEM = size_t(4) * PS * 4;
+	__device__ __forceinline__ static int addr(int k, int c) { return k * RS + (c & 7) * Q + (c >> 3); }
+};
+
+// Last LR inverse stages (normalisation folded in), then per 8-coefficient
+// segment: CRT of the four primes, base-b digits through the window, and the
+// segment's PK_CARRY carries.
+template <int LR>
+__device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, bool dup, uint32_t *sm)
+{
+	using S = PColShape<LR>;
+	constexpr int R = S::R, T = S::T, PS = S::PS, SPR = T / (SEG / 2);
+	const size_t Np = size_t(1) << a.n, Cp = size_t(1) << (a.n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x;
+	for_planes<2>([&](auto PLc) {
+		constexpr int PL = decltype(PLc)::value;
+		using Z = ZS<2, PL>;
+		const uint32_t *src = d.planes + PL * Np + c0 + tid;
+		uint32_t x[R];
+#pragma unroll
+		for (int k = 0; k < R; ++k) x[k] = src[k * Cp];
+		inv_reg<Z, LR>(Z{}, x, 1u, a.tab[2].iv[PL], true, __ldg(&a.tab[2].fw[PL][0]), __ldg(&a.tab[2].iv[PL][0]));
+#pragma unroll
+		for (int k = 0; k < R; ++k) sm[PL * PS + S::addr(k, tid)] = x[k];
+	});
+	__syncthreads();
+	int32_t *out = d.regs + static_cast<size_t>(a.dst) * (2 * Np);
+	for (int e = tid; e < R * SPR; e += T)
+	{
+		const int k = e / SPR, s = e % SPR;
+		const size_t i0 = static_cast<size_t>(k) * Cp + c0 + static_cast<size_t>(s) * (SEG / 2);
+		int64_t win[7] = { 0, 0, 0, 0, 0, 0, 0 };
+		int32_t dg[SEG];
+#pragma unroll
+		for (int ci = 0; ci < SEG / 2; ++ci)
+		{
+			uint32_t x[4];
+#pragma unroll
+			for (int pl = 0; pl < 4; ++pl) x[pl] = sm[pl * PS + S::addr(k, s * (SEG / 2) + ci)];
+			crt_window(x, dup ? 1 : 0, d.ck, d.pk, win);
+			dg[2 * ci] = window_digit(d.ck, win);
+			dg[2 * ci + 1] = window_digit(d.ck, win);
+		}
+		int4 *o = reinterpret_cast<int4 *>(out + 2 * i0);
+#pragma unroll
+		for (int i = 0; i < SEG / 4; ++i) o[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
+		int64_t *cs = d.carry + PK_CARRY * (i0 / (SEG / 2));
+#pragma unroll
+		for (int q = 0; q < PK_CARRY; ++q) cs[q] = win[q];
+	}
+}
+
+template <int LR>
+__global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_fwd(const Args a)
+{
+	__shared__ int32_t sm[(1 << LR) * (2 * PCOL_THREADS + 2)];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	pcol_fwd_body<LR>(a, d, sm);
+}
+
+template <int LR>
+__global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_inv(const Args a)
+{
+	extern __shared__ __align__(16) uint32_t sm[];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	const bool dup = get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	pcol_inv_body<LR>(a, d, dup, sm);
+}
+
+// Pending packed carries of register a.dst absorbed (a.n = n: digits).
+__global__ void __launch_bounds__(256) k_pfixup(const Args a)
+{
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	const size_t N = size_t(1) << a.n;
+	const size_t nseg = N / SEG;
+	const size_t s = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (s >= nseg) return;
+	int64_t c[PK_CARRY];
+	take_carry5(d, s, nseg, c);
+	bool any = false;
+#pragma unroll
+	for (int k = 0; k < PK_CARRY; ++k) any |= (c[k] != 0);
+	if (!any) return;
+	int4 *p = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(a.dst) * N + s * SEG);
+	int32_t dg[SEG];
+#pragma unroll
+	for (int i = 0; i < SEG / 4; ++i)
+	{
+		const int4 v = p[i];
+		dg[4 * i] = v.x; dg[4 * i + 1] = v.y; dg[4 * i + 2] = v.z; dg[4 * i + 3] = v.w;
+	}
+	if (!absorb5<SEG>(dg, c, d.ck)) atomicOr(a.err, 1u);
+#pragma unroll
+	for (int i = 0; i < SEG / 4; ++i) p[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
 }
 
 // Each segment absorbs the carry of the previous one (segment 0 takes minus

@@ -168,8 +168,12 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
  * state in the cluster's shared memory (15 <= n <= 17; products use the
  * default four-step plan); 3 <= lr <= 10: four-step with R = 2^lr rows
  * (8 <= n - lr <= 13); lr = 100 + lr2 (3 <= lr2 <= 7): six-step, the column
- * transform split into 2^4 and 2^lr2 points (8 <= n - 4 - lr2 <= 13).
- * gfc_batch_plan reads the current plan. */
+ * transform split into 2^4 and 2^lr2 points (8 <= n - 4 - lr2 <= 13);
+ * lr = 200 + l (l = 3, 4): packed digits, two base-b digits per coefficient
+ * of a transform of N/2 points over four primes (8 <= n - 1 - l <= 13; every
+ * base of the batch in the exact range, 2^20 <= b and (N/2)((b/2+1)(b+1))^2
+ * below half the primes' product, else GFC_ERR_RANGE; gfc_batch_widths then
+ * reports 4).  gfc_batch_plan reads the current plan. */
 int gfc_batch_set_plan(gfc_batch *bt, int lr);
 int gfc_batch_plan(const gfc_batch *bt);
 
