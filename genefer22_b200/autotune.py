@@ -4,9 +4,10 @@ A plan is the split of the length-N transform: ``lr = 0`` keeps a whole test
 in one CTA's shared memory (n <= 14); ``lr = 1`` keeps it in the shared
 memory of a thread-block cluster of 2^(n-13) CTAs (15 <= n <= 17); ``100 +
 lr2`` splits the column transform into a 16-point register pass and a
-2^lr2-point middle pass (six-step); ``200 + lr`` packs two base-b digits into
-one coefficient of a half-length transform over four primes (valid when every
-base of the batch lies in the exact range; the engine refuses it otherwise);
+2^lr2-point middle pass (six-step); ``200 + lr`` (four-step) and ``300 + lr2`` (six-step)
+pack two base-b digits into one coefficient of a half-length transform over
+four primes (valid when every base of the batch lies in the exact range; the
+engine refuses it otherwise);
 ``lr >= 3`` runs the four-step form,
 2^lr-point column transforms (radix-16 register groups, 2^lr-point tiles in
 shared memory or registers) then 2^(n - lr)-point row transforms, the row
@@ -44,6 +45,7 @@ SMALL_MAX_LOGN = 14
 PLAN_CLUSTER = 1
 PLAN_SIX = 100
 PLAN_PACKED = 200
+PLAN_PACKED_SIX = 300
 
 
 def candidates(n: int) -> List[int]:
@@ -58,6 +60,10 @@ def candidates(n: int) -> List[int]:
     for lr in (3, 4):                       # packed digits: four primes, transform of N/2
         if 8 <= n - 1 - lr <= 13:
             out.append(PLAN_PACKED + lr)
+    for lr2 in range(3, 8):                 # packed digits, six-step on N/2
+        lc = n - 1 - 4 - lr2
+        if 8 <= lc <= 13 and max(32, 4096 >> lr2) <= (1 << lc):
+            out.append(PLAN_PACKED_SIX + lr2)
     for lr2 in range(3, 8):                 # six-step: 2^4 x 2^lr2 column split
         lc = n - 4 - lr2
         if 8 <= lc <= 13 and max(32, 4096 >> lr2) <= (1 << lc):

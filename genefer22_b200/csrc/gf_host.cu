@@ -426,37 +426,49 @@ void launch_cluster_lq(int lq, const Args &a, int ntests, int max_active, cudaSt
 
 // Six-step middle pass (k_mid): planes of every test, tiles of 2^lr2 rows.
 template <int LR2>
-void mid_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+void mid_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 {
 	using S = ColShape<LR2>;
-	if (prep) { set_smem(k_mid<LR2, false>, S::SMEM); set_smem(k_mid<LR2, true>, S::SMEM); return; }
+	const size_t smem = size_t(planes) * S::PS * 4;
+	if (prep)
+	{
+		set_smem(k_mid<LR2, false>, size_t(4) * S::PS * 4);
+		set_smem(k_mid<LR2, true>, size_t(4) * S::PS * 4);
+		return;
+	}
 	const size_t C = size_t(1) << (a.n - MID_LR1 - LR2);
 	const dim3 grid(static_cast<unsigned>((size_t(1) << MID_LR1) * (C / S::CW)), static_cast<unsigned>(grid_y));
-	if (inv) k_mid<LR2, true><<<grid, col_threads(LR2), S::SMEM, s>>>(a);
-	else k_mid<LR2, false><<<grid, col_threads(LR2), S::SMEM, s>>>(a);
+	if (inv) k_mid<LR2, true><<<grid, col_threads(LR2), smem, s>>>(a);
+	else k_mid<LR2, false><<<grid, col_threads(LR2), smem, s>>>(a);
 	after_launch();
 }
 
-void launch_mid(int lr2, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
+void launch_mid(int lr2, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep, int planes = 3)
 {
 	switch (lr2)
 	{
-		case 3: mid_t<3>(inv, a, grid_y, s, prep); break;
-		case 4: mid_t<4>(inv, a, grid_y, s, prep); break;
-		case 5: mid_t<5>(inv, a, grid_y, s, prep); break;
-		case 6: mid_t<6>(inv, a, grid_y, s, prep); break;
-		case 7: mid_t<7>(inv, a, grid_y, s, prep); break;
+		case 3: mid_t<3>(inv, a, grid_y, s, prep, planes); break;
+		case 4: mid_t<4>(inv, a, grid_y, s, prep, planes); break;
+		case 5: mid_t<5>(inv, a, grid_y, s, prep, planes); break;
+		case 6: mid_t<6>(inv, a, grid_y, s, prep, planes); break;
+		case 7: mid_t<7>(inv, a, grid_y, s, prep, planes); break;
 		default: fail(GFC_ERR_ARG, "six-step plan needs 3 <= lr2 <= 7");
 	}
 }
 
 constexpr int PLAN_SIX = 100;     // plan codes 100 + lr2: six-step, 2^4 x 2^lr2 column split
 constexpr int PLAN_PACKED = 200;  // plan codes 200 + lr: packed digits, four-step of n - 1 with lr = 3, 4
+constexpr int PLAN_PACKED_SIX = 300;   // plan codes 300 + lr2: packed digits, six-step of n - 1
 
 constexpr int PLAN_CLUSTER = 1;   // plan code of the cluster-resident squaring
 
 bool plan_valid(int n, int lr)
 {
+	if (lr > PLAN_PACKED_SIX)
+	{
+		const int lr2 = lr - PLAN_PACKED_SIX, lc = n - 1 - MID_LR1 - lr2;
+		return (lr2 >= 3) && (lr2 <= 7) && (lc >= 8) && (lc <= 13) && (col_width(lr2) <= (1 << lc));
+	}
 	if (lr > PLAN_PACKED)
 	{
 		const int l = lr - PLAN_PACKED, lc = n - 1 - l;
@@ -476,6 +488,17 @@ bool plan_valid(int n, int lr)
 // Default plan code: single-CTA up to n = 14, four-step with rows of 2^12
 // (fewer below n = 15), six-step with rows of 2^12 from n = 21, where a
 // 2^(n-12)-point column tile would leave one or two CTAs per SM.
+// Default plan of a batch of at least 2^21 digits whose bases all fit packed
+// digits (n >= 17):
+// four-step on N/2 with 16-row columns up to n = 18, six-step on N/2 above
+// (measured fastest per n on one B200).
+int default_packed_plan(int n)
+{
+	if (n <= 18) return PLAN_PACKED + 4;
+	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 4, 6, 6 };
+	return PLAN_PACKED_SIX + lr2[n];
+}
+
 int default_plan(int n)
 {
 	if (n <= SMALL_MAX_LOGN) return 0;
@@ -578,7 +601,13 @@ void apply_plan(gfc_batch &bt, int code)
 	bt.cluster = 0;
 	bt.six = 0;
 	bt.packed = false;
-	if (code > PLAN_PACKED)
+	if (code > PLAN_PACKED_SIX)
+	{
+		bt.packed = true;
+		bt.six = code - PLAN_PACKED_SIX;
+		bt.lr = MID_LR1 + bt.six;
+	}
+	else if (code > PLAN_PACKED)
 	{
 		bt.packed = true;
 		bt.lr = code - PLAN_PACKED;
@@ -654,7 +683,8 @@ void prepare_plan(gfc_batch &bt)
 	if (bt.cluster > 0) launch_cluster_lq(bt.cluster, a, 0, 0, nullptr, true, &bt.cluster_max);
 	if (bt.packed)
 	{
-		launch_pcol(bt.lr, true, a, 0, nullptr, true);
+		launch_pcol(bt.six ? MID_LR1 : bt.lr, true, a, 0, nullptr, true);
+		if (bt.six) launch_mid(bt.six, false, a, 0, nullptr, true);
 		launch_row(bt.n - 1 - bt.lr, a, 0, nullptr, true);
 	}
 	else if (bt.lr == 0) launch_small(bt, a, nullptr, true);
@@ -687,7 +717,13 @@ Args packed_args(const gfc_batch &bt, const Args &a)
 
 void launch_cols_fwd(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
 {
-	if (bt.packed) { launch_pcol(bt.lr, false, packed_args(bt, a), g, s, false); return; }
+	if (bt.packed)
+	{
+		const Args p = packed_args(bt, a);
+		launch_pcol(bt.six ? MID_LR1 : bt.lr, false, p, g, s, false);
+		if (bt.six) launch_mid(bt.six, false, p, g, s, false, 4);
+		return;
+	}
 	if (bt.six == 0) { launch_col(bt.lr, false, a, g, s, false); return; }
 	launch_col(MID_LR1, false, a, g, s, false);
 	launch_mid(bt.six, false, a, g, s, false);
@@ -695,7 +731,13 @@ void launch_cols_fwd(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
 
 void launch_cols_inv(gfc_batch &bt, const Args &a, int g, cudaStream_t s)
 {
-	if (bt.packed) { launch_pcol(bt.lr, true, packed_args(bt, a), g, s, false); return; }
+	if (bt.packed)
+	{
+		const Args p = packed_args(bt, a);
+		if (bt.six) launch_mid(bt.six, true, p, g, s, false, 4);
+		launch_pcol(bt.six ? MID_LR1 : bt.lr, true, p, g, s, false);
+		return;
+	}
 	if (bt.six == 0) { launch_col(bt.lr, true, a, g, s, false); return; }
 	launch_mid(bt.six, true, a, g, s, false);
 	launch_col(MID_LR1, true, a, g, s, false);
@@ -993,6 +1035,15 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 	std::vector<int64_t> pos(count, -1);
 	GFC_CK(cudaMemcpyAsync(bt->d_pos, pos.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, bt->stream));
 	GFC_CK(cudaStreamSynchronize(bt->stream));
+	// packed digits halve the transform's parallelism: the default for batches
+	// of at least 2^21 digits (measured crossover at n = 17 .. 21)
+	bool packable = (bt->n >= 17) && ((size_t(count) << bt->n) >= (size_t(1) << 21));
+	for (size_t i = 0; packable && (i < count); ++i) packable = packed_ok(b[i], bt->n);
+	if (packable)
+	{
+		set_packed(*bt, true);
+		apply_plan(*bt, default_packed_plan(bt->n));
+	}
 	prepare_plan(*bt);
 	return bt.release();
 }
@@ -1132,7 +1183,11 @@ GFC_API int gfc_read_context(gfc_transform *t, const void *buf, size_t size, siz
 	});
 }
 
-GFC_API int gfc_width(const gfc_transform *t) { return (t == nullptr) ? GFC_ERR_ARG : (t->set[0] == 0 ? 2 : 3); }
+GFC_API int gfc_width(const gfc_transform *t)
+{
+	if (t == nullptr) return GFC_ERR_ARG;
+	return t->packed ? 4 : (t->set[0] == 0 ? 2 : 3);
+}
 
 GFC_API int gfc_sync(gfc_transform *t)
 {
@@ -1344,7 +1399,7 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 	return guard([&] {
 		GFC_NULLCHK(bt);
 		if (!plan_valid(bt->n, lr)) fail(GFC_ERR_ARG, "set_plan: invalid plan for this n");
-		const bool packed = lr > PLAN_PACKED;
+		const bool packed = lr > PLAN_PACKED;   // plans 200 + lr and 300 + lr2
 		if (packed)
 			for (size_t i = 0; i < bt->count; ++i)
 				if (!packed_ok(bt->b[i], bt->n)) fail(GFC_ERR_RANGE, "set_plan: a base is outside the range of packed digits");
@@ -1361,7 +1416,7 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 GFC_API int gfc_batch_plan(const gfc_batch *bt)
 {
 	if (bt == nullptr) return GFC_ERR_ARG;
-	if (bt->packed) return PLAN_PACKED + bt->lr;
+	if (bt->packed) return (bt->six > 0) ? PLAN_PACKED_SIX + bt->six : PLAN_PACKED + bt->lr;
 	if (bt->cluster > 0) return PLAN_CLUSTER;
 	return (bt->six > 0) ? PLAN_SIX + bt->six : bt->lr;
 }

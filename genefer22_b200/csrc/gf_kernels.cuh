@@ -918,7 +918,9 @@ __global__ void __launch_bounds__(col_threads(LR2)) k_mid(const Args a)
 	bool active;
 	(void)get_dup(a, d, t, a.j, active);
 	if (!active) return;
-	if (d.set == 0) mid_body<0, LR2, INV>(a, d, sm); else mid_body<1, LR2, INV>(a, d, sm);
+	if (d.set == 0) mid_body<0, LR2, INV>(a, d, sm);
+	else if (d.set == 1) mid_body<1, LR2, INV>(a, d, sm);
+	else mid_body<2, LR2, INV>(a, d, sm);
 }
 
 // ---- four-step with R <= 16 rows: one thread owns a whole column.

@@ -103,8 +103,11 @@ size_t gfc_context_size(const gfc_transform *t, size_t num_regs);
 int gfc_save_context(gfc_transform *t, void *buf, size_t size, size_t num_regs);
 int gfc_read_context(gfc_transform *t, const void *buf, size_t size, size_t num_regs);
 
-/* Number of RNS primes (2 or 3) chosen for (b, n); the analogue of the
- * transform kind NTT2/NTT3 (src/transform.h:45, src/transform_ocl.cpp:35-50). */
+/* Number of RNS primes chosen for (b, n): 2 or 3, or 4 with packed digits
+ * (two digits per coefficient of a half-length transform; the default from
+ * n = 21 for a single test whose b is in the packed range); the analogue of
+ * the transform kind
+ * NTT2/NTT3 (src/transform.h:45, src/transform_ocl.cpp:35-50). */
 int gfc_width(const gfc_transform *t);
 
 /* Waits for all enqueued work; returns GFC_ERR_NUMERIC if a device-side check
@@ -173,7 +176,12 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
  * of a transform of N/2 points over four primes (8 <= n - 1 - l <= 13; every
  * base of the batch in the exact range, 2^20 <= b and (N/2)((b/2+1)(b+1))^2
  * below half the primes' product, else GFC_ERR_RANGE; gfc_batch_widths then
- * reports 4).  gfc_batch_plan reads the current plan. */
+ * reports 4); lr = 300 + lr2: packed digits with the six-step split of the
+ * half-length transform (8 <= n - 5 - lr2 <= 13).  A new batch of at least
+ * 2^21 digits uses packed digits from n = 17 when every base is in the packed
+ * range, otherwise
+ * single-CTA up to n = 14, four-step up to n = 20, six-step above.
+ * gfc_batch_plan reads the current plan. */
 int gfc_batch_set_plan(gfc_batch *bt, int lr);
 int gfc_batch_plan(const gfc_batch *bt);
 

@@ -55,6 +55,27 @@ def test_packed_vs_oracle(oracle, n, plan, b):
     assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), "mul 2"
 
 
+@pytest.mark.parametrize("n,plan,b", [(18, 304, 100_000_002), (20, 305, 50_000_000), (22, 305, 35_000_000),
+                                      (23, 306, 25_000_002)])
+def test_packed_six_step_vs_oracle(oracle, n, plan, b):
+    """Packed digits with the six-step split of the half-length transform."""
+    rng = np.random.default_rng(n + 7)
+    t = Transform(b, n)
+    t.batch.set_plan(plan)
+    assert t.batch.plan() == plan
+    o = oracle.OracleTransform(b, n)
+    d = rand_digits(rng, b, 1 << n)
+    t.setInt(d)
+    o.setInt(d)
+    for dup in (False, True):
+        t.squareDup(dup)
+        o.squareDup(dup)
+        assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), dup
+    t.copy(1, 0); o.copy(1, 0)
+    t.mul(1); o.mul(1)
+    assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), "mul"
+
+
 def test_range_refused():
     for b in (2**20 - 2, B_MAX[16] + 2):
         bt = Batch([b, 2_000_002], 16)
