@@ -174,18 +174,34 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ GPU arm
 
+def plan_geometry(n: int, plan: int):
+    """(log2 of the transform length, log2 of the column length) of a plan:
+    packed plans (200 + lr, 300 + lr2) transform N/2 points; six-step plans
+    (100 + lr2, 300 + lr2) have columns of 2^(4 + lr2)."""
+    if plan > 300:
+        return n - 1, 4 + plan - 300
+    if plan > 200:
+        return n - 1, plan - 200
+    if plan > 100:
+        return n, 4 + plan - 100
+    return n, plan
+
+
 def algorithmic(kind: int, widths: np.ndarray, n: int, lr: int):
     """Algorithmic DRAM bytes and radix-2 butterflies of one launch of kernel
-    kind `kind` (see Batch.time_kernels) over all tests of the batch."""
+    kind `kind` (see Batch.time_kernels) over all tests of the batch.  n and
+    lr are those of the transform (n - 1 for packed digits, whose N/2
+    coefficients each carry two digits)."""
     N = 1 << n
     W = widths.astype(np.float64)
     lc = n - lr
+    dig = 4 * N * (2 if int(W[0]) == 4 else 1)      # digit bytes: two digits per packed coefficient
     if kind == 1:   # column forward: read digits, write W planes; lr stages
-        return float(np.sum(4 * N + 4 * W * N)), float(np.sum(W * (N / 2) * lr))
+        return float(np.sum(dig + 4 * W * N)), float(np.sum(W * (N / 2) * lr))
     if kind == 2:   # rows: read + write W planes; 2 lc stages + pointwise
         return float(np.sum(8 * W * N)), float(np.sum(W * (N / 2) * 2 * lc + W * N))
     if kind == 3:   # column inverse + CRT + carry: read W planes, write digits and carries
-        return float(np.sum(4 * W * N + 4 * N + 8 * N / 16)), float(np.sum(W * (N / 2) * lr))
+        return float(np.sum(4 * W * N + dig + 8 * (dig // 4) / 16)), float(np.sum(W * (N / 2) * lr))
     if kind == 4:   # carry fix-up: read carries
         return float(np.sum(8 * N / 16 + 0 * W)), 0.0
     # single-CTA squaring: digits in and out; the whole transform in shared memory
@@ -205,8 +221,10 @@ def run_ours(args):
     from genefer22_b200 import genefer as gf
 
     L = _lib.lib()
+    from genefer22_b200.autotune import Autotuner
     bs = bases(SEED + rank)
     bt = Batch(bs, N_LOG, num_regs=3, device=local)
+    tuned = Autotuner(squarings=16, replays=3).tune(bt)      # plan per size class, as production batches run
     widths = bt.widths()
     runner = gf.BatchPRP(bt, B=BLOCK)
     runner.load()
@@ -274,16 +292,17 @@ def run_ours(args):
 
     # per-kernel durations (CUDA events on the batch's stream) -> roofline of the dominant kernel
     lr = bt.plan()
+    n_t, lr_t = plan_geometry(N_LOG, lr)
     bt.time_kernels(2)                 # first launches of each kernel kind load it
     kms = bt.time_kernels(5)
     dom = int(np.argmax(kms[:4]))      # the stand-alone fix-up is not part of a graph step
     names = ["k_small", "k_col_fwd", "k_row", "k_col_inv", "k_fixup"]
-    abytes, abfly = algorithmic(dom, widths, N_LOG, lr)
+    abytes, abfly = algorithmic(dom, widths, n_t, lr_t)
     hbm, hbm_kind = peaks()
     achieved = abytes / (kms[dom] * 1e-3) / 1e9
     probe = (ctypes.c_double * 4)()
     L.gfc_probe_int_throughput(local, probe)
-    frac_w3 = float(np.mean(widths == 3))
+    frac_w3 = float(np.mean(widths >= 3))       # 31-bit primes (3 or 4 of them) vs 32-bit (2)
     bfly_peak = frac_w3 * probe[3] + (1 - frac_w3) * probe[2]
     traffic = None
     tj = os.path.join(ROOT, "profiles", "traffic.json")
@@ -318,7 +337,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": N_LOG, "tests_per_gpu": COUNT, "block": BLOCK, "seed": SEED,
-                   "plan_lr": lr, "rns_widths": {"2": int(np.sum(widths == 2)), "3": int(np.sum(widths == 3))},
+                   "plan": lr, "plan_us_per_squaring": {str(k): round(v, 1) for k, v in tuned.us.items()},
+                   "rns_widths": {str(w): int(np.sum(widths == w)) for w in sorted(set(widths.tolist()))},
                    "l2": "256 MB buffer written between timed steps", "graph": "one CUDA graph per block"},
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": traffic,
@@ -503,7 +523,8 @@ def run_sizes(args):
         plain = _plain_rate(bs[0], n, 100 if n <= 18 else 30)
         W = bt.widths()
         sq_ms = ms / blk
-        alg_bytes = float(np.sum(16 * W * (1 << n)))
+        n_t, _ = plan_geometry(n, tr.lr)                  # packed plans: W = 4 planes of N/2
+        alg_bytes = float(np.sum(16 * W * (1 << n_t)))
         out[n] = {"tests": count, "plan_lr": tr.lr, "widths": sorted(set(int(w) for w in W)),
                   "batched": batched, "plain": plain, "batched_over_plain": batched / plain,
                   "us_per_batch_squaring": sq_ms * 1e3,

@@ -330,15 +330,15 @@ void launch_col(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, boo
 	}
 }
 
-// Rows of 2^LC points; `planes` = 3, or 4 for packed digits (prime set 2),
-// sets the shared memory of the launch.
+// Rows of 2^LC points, one (row, plane) per CTA; `planes` = 3, or 4 for
+// packed digits (prime set 2).
 template <int LC>
 void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 {
 	using S = RowShape<LC>;
-	const size_t smem = size_t(planes) * S::PC * 4;
-	if (prep) { set_smem(k_row<LC>, size_t(4) * S::PC * 4); return; }
-	const dim3 grid(1u << (a.n - LC), static_cast<unsigned>(grid_y));
+	const size_t smem = size_t(S::PC) * 4;          // one plane per CTA
+	if (prep) { set_smem(k_row<LC>, smem); return; }
+	const dim3 grid((1u << (a.n - LC)) * static_cast<unsigned>(planes), static_cast<unsigned>(grid_y));
 	k_row<LC><<<grid, row_threads(LC), smem, s>>>(a);
 	after_launch();
 }

@@ -200,7 +200,8 @@ enum : int { IO_SMEM = 0, IO_GIN = 1, IO_GOUT = 2 };
 template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO = IO_SMEM>
 __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										 uint32_t base_step, const Tables &tab, const uint32_t *__restrict__ zrow,
-										 size_t zstride, uint32_t *gmem = nullptr, size_t gstride = 0)
+										 size_t zstride, uint32_t *gmem = nullptr, size_t gstride = 0, int pl_lo = 0,
+										 int pl_hi = PrimeSet<SET>::W)
 {
 	constexpr int W = PrimeSet<SET>::W;
 	constexpr int E = 1 << r;
@@ -216,10 +217,10 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 		const uint32_t tb = ((base0 + static_cast<uint32_t>(lane) * base_step) << SIGMA) + G.blk;
 		const int base = Map::addr(G.i0, lane);
 #pragma unroll 1
-		for (int pl = 0; pl < W; ++pl)
+		for (int pl = pl_lo; pl < pl_hi; ++pl)
 		{
 			const auto z = prime_rt<SET>(pl);
-			uint32_t *pb = buf + pl * pstride + base;
+			uint32_t *pb = buf + (pl - pl_lo) * pstride + base;
 			uint32_t *gb = gmem;
 			if constexpr (IO != IO_SMEM) gb = gmem + pl * gstride + (static_cast<size_t>(lane) << L) + G.i0;
 			uint32_t x[E];
@@ -264,13 +265,13 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 // Forward passes 0 .. NP-1 (or NP-2 with SKIP_LAST), a barrier after each.
 template <int SET, int L, bool SKIP_LAST, class Map>
 __device__ __forceinline__ void run_fwd(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
-										uint32_t base_step, const Tables &tab)
+										uint32_t base_step, const Tables &tab, int pl_lo = 0, int pl_hi = PrimeSet<SET>::W)
 {
 	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
 	static_for<0, NP>([&](auto P) {
 		constexpr int p = decltype(P)::value;
 		pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
-															  nullptr, 0);
+															  nullptr, 0, nullptr, 0, pl_lo, pl_hi);
 		__syncthreads();
 	});
 }
@@ -278,13 +279,13 @@ __device__ __forceinline__ void run_fwd(uint32_t *buf, int pstride, int lanes_lo
 // Inverse passes NP-1 (or NP-2 with SKIP_LAST) .. 0.
 template <int SET, int L, bool SKIP_LAST, class Map>
 __device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
-										uint32_t base_step, const Tables &tab)
+										uint32_t base_step, const Tables &tab, int pl_lo = 0, int pl_hi = PrimeSet<SET>::W)
 {
 	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
 	static_for<0, NP>([&](auto Q) {
 		constexpr int p = NP - 1 - decltype(Q)::value;
 		pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
-															  nullptr, 0);
+															  nullptr, 0, nullptr, 0, pl_lo, pl_hi);
 		__syncthreads();
 	});
 }
@@ -295,7 +296,8 @@ __device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_lo
 // Squaring or product only (not OP_FWD).
 template <int SET, int L, class Map>
 __device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint32_t base0, const Tables &tab,
-												const uint32_t *zrow, size_t zstride, int op, uint32_t *g, size_t gstride)
+												const uint32_t *zrow, size_t zstride, int op, uint32_t *g, size_t gstride,
+												int pl_lo, int pl_hi)
 {
 	constexpr int NP = Sched<L>::NP;
 	static_assert(NP >= 2, "rows of at least two passes");
@@ -303,25 +305,29 @@ __device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint
 		constexpr int p = decltype(P)::value;
 		if constexpr (p == 0)
 			pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map, IO_GIN>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
-																		  g, gstride);
+																		  g, gstride, pl_lo, pl_hi);
 		else
-			pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0);
+			pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
+																  nullptr, 0, pl_lo, pl_hi);
 		__syncthreads();
 	});
 	constexpr int PL = NP - 1;
 	if (op == OP_MUL)
-		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride);
+		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride,
+																	nullptr, 0, pl_lo, pl_hi);
 	else
-		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride);
+		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride,
+																   nullptr, 0, pl_lo, pl_hi);
 	__syncthreads();
 	static_for<0, NP - 1>([&](auto Q) {
 		constexpr int p = NP - 2 - decltype(Q)::value;
 		if constexpr (p == 0)
 			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_GOUT>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
-																		   g, gstride);
+																		   g, gstride, pl_lo, pl_hi);
 		else
 		{
-			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0);
+			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
+																  nullptr, 0, pl_lo, pl_hi);
 			__syncthreads();
 		}
 	});
@@ -733,6 +739,11 @@ __device__ __forceinline__ void col_fwd_body(const Args &a, const TestDesc &d, u
 	}
 }
 
+// One plane of one row per CTA: blockIdx.x = row * P + plane, P = planes of
+// the launch (3, or 4 with packed digits); a CTA whose plane the test does not
+// have returns.  The planes of a row are independent until the CRT, so a CTA
+// holds one plane (shared memory PC words) and an SM holds as many CTAs as
+// its registers allow.
 template <int SET, int LC>
 __device__ __forceinline__ void row_body(const Args &a, const TestDesc &d, uint32_t *sm)
 {
@@ -740,34 +751,32 @@ __device__ __forceinline__ void row_body(const Args &a, const TestDesc &d, uint3
 	constexpr int W = PrimeSet<SET>::W;
 	const int n = a.n, lr = n - LC;
 	const size_t N = size_t(1) << n;
-	const int k = blockIdx.x;             // one row per CTA
+	const int P = static_cast<int>(gridDim.x >> lr);
+	const int k = static_cast<int>(blockIdx.x) / P, pl = static_cast<int>(blockIdx.x) % P;
+	if (pl >= W) return;
 	uint32_t *buf = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(k) * S::C;
+	const uint32_t base = (1u << lr) + static_cast<uint32_t>(k);
 	using MP = RowMap<LC>;
 
 	if (a.op != OP_FWD)
 	{
-		row_core_global<SET, LC, MP>(sm, S::PC, (1u << lr) + static_cast<uint32_t>(k), a.tab[SET],
-									 d.zp + static_cast<size_t>(k) * S::C, N, a.op, buf, N);
+		row_core_global<SET, LC, MP>(sm, S::PC, base, a.tab[SET], d.zp + static_cast<size_t>(k) * S::C, N, a.op, buf, N,
+									 pl, pl + 1);
 		return;
 	}
-#pragma unroll
-	for (int pl = 0; pl < W; ++pl)
-		for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
-		{
-			const uint4 u = *reinterpret_cast<const uint4 *>(buf + pl * N + 4 * e);
-			uint32_t *p = sm + pl * S::PC + MP::addr(4 * e, 0);
-			p[0] = u.x; p[1] = u.y; p[2] = u.z; p[3] = u.w;
-		}
+	for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
+	{
+		const uint4 u = *reinterpret_cast<const uint4 *>(buf + pl * N + 4 * e);
+		uint32_t *p = sm + MP::addr(4 * e, 0);
+		p[0] = u.x; p[1] = u.y; p[2] = u.z; p[3] = u.w;
+	}
 	__syncthreads();
-	row_core<SET, LC, MP>(sm, S::PC, 0, (1u << lr) + static_cast<uint32_t>(k), a.tab[SET],
-						  d.zp + static_cast<size_t>(k) * S::C, N, a.op);
-#pragma unroll
-	for (int pl = 0; pl < W; ++pl)
-		for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
-		{
-			const uint32_t *p = sm + pl * S::PC + MP::addr(4 * e, 0);
-			*reinterpret_cast<uint4 *>(buf + pl * N + 4 * e) = make_uint4(p[0], p[1], p[2], p[3]);
-		}
+	run_fwd<SET, LC, false, MP>(sm, S::PC, 0, false, base, 1u, a.tab[SET], pl, pl + 1);
+	for (int e = threadIdx.x; e < S::C / 4; e += blockDim.x)
+	{
+		const uint32_t *p = sm + MP::addr(4 * e, 0);
+		*reinterpret_cast<uint4 *>(buf + pl * N + 4 * e) = make_uint4(p[0], p[1], p[2], p[3]);
+	}
 }
 
 template <int SET, int LR>
