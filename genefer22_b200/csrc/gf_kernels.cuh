@@ -663,7 +663,9 @@ constexpr int FS_THREADS = 256;
 // Threads per CTA: a shared-memory tile that leaves room for one or two CTAs
 // on an SM gets more threads, so that every SM still holds 32 warps.
 __host__ __device__ constexpr int col_threads(int lr) { return (lr >= 9) ? 1024 : ((lr == 8) ? 512 : FS_THREADS); }
-__host__ __device__ constexpr int row_threads(int lc) { return (lc >= 13) ? 512 : FS_THREADS; }
+// A row CTA transforms one plane: 2^(lc-4) radix-16 groups per pass, one per
+// thread (at least two warps).
+__host__ __device__ constexpr int row_threads(int lc) { return (lc >= 11) ? (1 << (lc - 4)) : 64; }
 
 template <int SET, int LR>
 __device__ __forceinline__ void col_fwd_body(const Args &a, const TestDesc &d, uint32_t *sm)
