@@ -48,6 +48,18 @@ PLAN_PACKED = 200
 PLAN_PACKED_SIX = 300
 
 
+# Prime set 2 of the engine (packed digits): the exact range of plans 200 + lr
+# and 300 + lr2 (the engine refuses other bases with GFC_ERR_RANGE).
+_P2 = (127 * 2**24 + 1, 63 * 2**25 + 1, 249 * 2**23 + 1, 15 * 2**27 + 1)
+_M2 = _P2[0] * _P2[1] * _P2[2] * _P2[3]
+
+
+def packed_ok(b: int, n: int) -> bool:
+    """Whether base b at size n fits packed digits (two per coefficient)."""
+    b = int(b)
+    return (1 << 20) <= b < (1 << 28) and ((b // 2 + 1) * (b + 1)) ** 2 < (_M2 // 2) // (1 << (int(n) - 1))
+
+
 def candidates(n: int) -> List[int]:
     """Plans the engine accepts for size n (it rejects the others with GFC_ERR_ARG)."""
     out = [0] if n <= SMALL_MAX_LOGN else []
@@ -79,12 +91,14 @@ class TuneResult:
     lr: int                         # chosen plan
     us: Dict[int, float] = field(default_factory=dict)   # plan -> microseconds per batch squaring
 
+    packable: bool = False
+
     def key(self) -> str:
-        return key(self.n, self.count, self.wide)
+        return key(self.n, self.count, self.wide, self.packable)
 
 
-def key(n: int, count: int, wide: int) -> str:
-    return f"n{n}_c{count}_w{wide}"
+def key(n: int, count: int, wide: int, packable: bool = False) -> str:
+    return f"n{n}_c{count}_w{wide}" + ("_p" if packable else "")
 
 
 class Autotuner:
@@ -124,12 +138,17 @@ class Autotuner:
 
     def tune(self, bt: Batch, force: bool = False) -> TuneResult:
         """Chooses and sets the fastest plan for bt (before its tests are loaded)."""
-        wide = int(np.count_nonzero(bt.widths() == 3))
-        k = key(bt.n, bt.count, wide)
+        packable = all(packed_ok(b, bt.n) for b in bt.bases)
+        wide = int(np.count_nonzero(bt.widths() >= 3))
+        k = key(bt.n, bt.count, wide, packable)
         if (not force) and (k in self.cache):
             c = self.cache[k]
-            bt.set_plan(int(c["lr"]))
-            return TuneResult(bt.n, bt.count, wide, int(c["lr"]), {int(a): v for a, v in c["us"].items()})
+            try:
+                bt.set_plan(int(c["lr"]))
+                return TuneResult(bt.n, bt.count, wide, int(c["lr"]), {int(a): v for a, v in c["us"].items()},
+                                  packable)
+            except GfcError:
+                pass                                  # a plan this batch cannot take: measure
         us: Dict[int, float] = {}
         for lr in candidates(bt.n):
             try:
@@ -143,4 +162,4 @@ class Autotuner:
         bt.set(0)
         self.cache[k] = {"lr": best, "us": {str(a): v for a, v in us.items()}}
         self._save()
-        return TuneResult(bt.n, bt.count, wide, best, us)
+        return TuneResult(bt.n, bt.count, wide, best, us, packable)

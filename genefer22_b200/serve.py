@@ -42,7 +42,7 @@ from typing import Deque, Dict, List, Optional, Sequence
 import numpy as np
 
 from . import gint
-from .autotune import Autotuner
+from .autotune import Autotuner, packed_ok
 from .exponent import chunk_sum
 from .genefer import Job, gl_validate
 from .transform import Batch
@@ -134,9 +134,25 @@ class _Budget:
         self.used -= nbytes + (table_bytes(n) if self.tables[n] == 0 else 0)
 
 
+# From this size, packed digits are faster even for pools of one or two tests
+# (measured); smaller sizes keep one kind of pool, so that requests are not
+# split between two half-full pools.
+PACKED_POOL_MIN_N = 19
+
+
+def _packed_pool(b: int, n: int) -> bool:
+    return (int(n) >= PACKED_POOL_MIN_N) and packed_ok(b, n)
+
+
 class _Pool:
-    def __init__(self, server: "Server", pid: int, n: int, capacity: int, nbytes: int):
+    """Slots of one size.  A pool opened (at n >= PACKED_POOL_MIN_N) for a base
+    in the packed range tunes with that base, so that packed plans are
+    candidates, and takes only such bases; any other pool takes every base."""
+
+    def __init__(self, server: "Server", pid: int, n: int, capacity: int, nbytes: int, rep_b: int = 1024):
         self.server, self.pid, self.n, self.capacity, self.nbytes = server, pid, n, capacity, nbytes
+        self.rep_b = int(rep_b)
+        self.packed_only = _packed_pool(rep_b, n)
         self.slots: List[Optional[_Active]] = [None] * capacity
         self.reserved = 0                       # admitted by the dispatcher, not yet loaded
         self.batch: Optional[Batch] = None
@@ -151,8 +167,7 @@ class _Pool:
     # -- runs on the pool's thread
     def _setup(self):
         srv = self.server
-        b0 = 1024
-        self.batch = Batch([b0] * self.capacity, self.n, num_regs=NUM_REGS, device=srv.device)
+        self.batch = Batch([self.rep_b] * self.capacity, self.n, num_regs=NUM_REGS, device=srv.device)
         if srv.tuner is not None:
             self.plan = srv.tuner.tune(self.batch).lr
         else:
@@ -281,11 +296,12 @@ class Server:
         q = self.waiting[pool.n]
         out = []
         for slot in range(pool.capacity):
-            if not q:
-                break
             if pool.slots[slot] is not None:
                 continue
-            req = q.popleft()
+            req = next((r for r in q if not pool.packed_only or _packed_pool(r.job.b, pool.n)), None)
+            if req is None:
+                break
+            q.remove(req)
             pool.reserved += 1
             c = Completion(req.id, req.job.b, req.job.n, req.job.nbits, req.arrival, admitted=self.clock(),
                            pool=pool.pid, slot=slot)
@@ -310,18 +326,30 @@ class Server:
         for n, q in self.waiting.items():
             if not q:
                 continue
-            free = sum(p.free_slots() for p in self.pools if p.n == n)
-            while free < len(q):
+            anyb = [r for r in q if not _packed_pool(r.job.b, n)]   # need a pool that takes every base
+            packb = [r for r in q if _packed_pool(r.job.b, n)]
+            free_any = sum(p.free_slots() for p in self.pools if p.n == n and not p.packed_only)
+            free_pk = sum(p.free_slots() for p in self.pools if p.n == n and p.packed_only)
+            while True:
+                if free_any < len(anyb):
+                    rep, is_pk = 1024, False
+                elif free_pk + (free_any - len(anyb)) < len(packb):
+                    rep, is_pk = packb[0].job.b, True
+                else:
+                    break
                 cap = max(1, int(self.capacity(n)))
                 nb = cap * (slot_bytes(n) + self._exp_bytes[n])
                 if not self.budget.take(n, nb):
                     break
-                p = _Pool(self, self._next_pid, n, cap, nb)
+                p = _Pool(self, self._next_pid, n, cap, nb, rep_b=rep)
                 self._next_pid += 1
                 self.pools.append(p)
                 self.stats.pools_created += 1
                 p.thread.start()
-                free += cap
+                if is_pk:
+                    free_pk += cap
+                else:
+                    free_any += cap
 
     # -------------------------------------------------- from pool threads
     def _finished(self, pool: _Pool, slot: int, act: _Active, x: np.ndarray, d: np.ndarray):
@@ -406,8 +434,10 @@ class Server:
             self.budget.limit -= vbytes
         if self.tuner is not None:               # plans chosen before the clock starts
             for n in ns:
-                with Batch([1024] * max(1, int(self.capacity(n))), n, num_regs=NUM_REGS, device=self.device) as bt:
-                    self.tuner.tune(bt)
+                reps = [1024] + [next((int(r.job.b) for r in reqs if int(r.job.n) == n and _packed_pool(r.job.b, n)), 1024)]
+                for rep in sorted(set(reps)):
+                    with Batch([rep] * max(1, int(self.capacity(n))), n, num_regs=NUM_REGS, device=self.device) as bt:
+                        self.tuner.tune(bt)
         self._t0 = time.perf_counter()
         vths = [threading.Thread(target=self._validator, args=(n,), name=f"validator-n{n}", daemon=True)
                 for n in ns] if self.validate else []

@@ -273,3 +273,12 @@ def test_serve_budget_too_small(fake_engine):
     reqs = _requests(4, count=2)
     with pytest.raises(ValueError):
         sv.Server(B=4, budget_bytes=1000).run(reqs)
+
+
+def test_packed_range():
+    """The packed-digit range the engine enforces (packed_ok in gf_host.cu)."""
+    from genefer22_b200.autotune import packed_ok
+    assert packed_ok(184393718, 16) and not packed_ok(184393720, 16)
+    assert packed_ok(130386048, 18) and not packed_ok(130386050, 18)
+    assert not packed_ok(2**20 - 2, 16) and packed_ok(2**20, 16)
+    assert not packed_ok(2**28, 12)
