@@ -491,6 +491,47 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_verify(args):
+    """One test at n = 20 (b even, seeded uniform in [1e6, 5e7], seed 1003) with a
+    Gerbicz-Li check every 2000 squarings (B = 200, spans of 10 blocks) and one
+    seeded single-bit fault (seed 1013) that the check detects and rolls back;
+    the first `steps` spans of the exponent, timed against the same spans
+    without checks (plain blocks of squarings)."""
+    import torch
+    from genefer22_b200.verify import VerifiedPRP, flip_bit
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(1003)
+    b = int(rng.integers(5 * 10**5, 25 * 10**6)) * 2
+    spans = max(2, args.steps)
+    at = int(np.random.default_rng(1013).integers(2000, 4000))
+    warm = VerifiedPRP(b, 20, B=200, span=10)
+    warm.run(max_spans=1)
+    v = VerifiedPRP(b, 20, B=200, span=10)
+    t0 = time.perf_counter()
+    v.run(fault=flip_bit(1013), fault_at=at, max_spans=spans)
+    dt = time.perf_counter() - t0
+    useful = spans * 2000 * (1 << 20)
+    # the same squarings without checks
+    bt = v.batch
+    bt.set(3)
+    bt.sync()
+    t1 = time.perf_counter()
+    bt.square(False, spans * 2000)
+    bt.sync()
+    plain_s = time.perf_counter() - t1
+    st = v.stats
+    line = {"metric": METRIC, "value": useful / dt, "unit": METRIC, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "one test n=20, b even uniform [1e6,5e7] seed 1003, Gerbicz-Li check every "
+                                   "2000 squarings (B=200, span 10), one seeded single-bit fault (seed 1013)",
+                       "b": b, "spans": spans, "fault_at_squaring": at, "plan": bt.plan()},
+            "checks": st.checks, "failures": st.failures, "rollbacks": st.rollbacks,
+            "squarings_done": st.squarings, "check_squarings": st.check_squarings,
+            "unchecked_value": useful / plain_s,
+            "overhead_vs_unchecked": dt / plain_s - 1.0}
+    print(json.dumps(line), flush=True)
+
+
 def run_sizes(args):
     """Per size n = 12..23: a batch (tests per launch as in serving pools) run as
     graph-replayed blocks vs the plain path (one test, one call per squaring)."""
@@ -543,7 +584,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="batch", choices=["batch", "uneven", "serve", "sizes"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "uneven", "serve", "sizes", "verify"],
                     help="batch: the default line; the others print their own line")
     ap.add_argument("--serve-requests", type=int, default=40)
     args = ap.parse_args()
@@ -557,6 +598,8 @@ def main():
         run_serve(args)
     elif args.workload == "sizes":
         run_sizes(args)
+    elif args.workload == "verify":
+        run_verify(args)
     else:
         run_ours(args)
 
