@@ -181,3 +181,29 @@ def test_packed_quick_residue():
     t2.batch.set_plan(203)
     r2 = gf.quick(t2)
     assert r2 == r1 and r2.gl_ok
+
+
+@pytest.mark.parametrize("n,plan", [(16, 203), (16, 204), (20, 304)])
+def test_packed_extreme_states(oracle, n, plan):
+    """Digits at the resting bound +-(b/2 + 1) at the largest packed base: the
+    half-length convolution reaches (N/2) ((b/2+1)(b+1))^2, next to the exact
+    range of the four primes, and the carry window its largest values."""
+    b = {16: B_MAX[16], 20: 55_000_000}[n]
+    N = 1 << n
+    h = b // 2 + 1
+    states = [np.full(N, h, np.int32), np.full(N, -h, np.int32),
+              np.where(np.arange(N) % 2 == 0, h, -h).astype(np.int32),
+              np.where((np.arange(N) // 2) % 2 == 0, h, -h).astype(np.int32)]
+    for d in states:
+        bt = Batch([b], n)
+        bt.set_plan(plan)
+        bt.put(0, d)
+        o = oracle.OracleTransform(b, n)
+        o.setInt(canon(d, b))
+        for dup in (False, True):
+            bt.square(dup, 1)
+            o.squareDup(dup)
+            got = bt.get(0)
+            assert np.abs(got).max() <= b // 2 + 1
+            assert np.array_equal(canon(got, b), canon(o.getInt(), b)), (int(d[0]), int(d[1]), dup)
+        bt.close()

@@ -282,3 +282,25 @@ def test_packed_range():
     assert packed_ok(130386048, 18) and not packed_ok(130386050, 18)
     assert not packed_ok(2**20 - 2, 16) and packed_ok(2**20, 16)
     assert not packed_ok(2**28, 12)
+
+
+def test_serve_packed_pools(fake_engine, oracle, monkeypatch):
+    """Pools of packed-range bases take only such bases, general pools take
+    every base; each request is served once and correctly."""
+    monkeypatch.setattr(sv, "PACKED_POOL_MIN_N", 8)
+    B = 6
+    reqs = []
+    rng = np.random.default_rng(21)
+    for i in range(8):
+        b = (2_000_002 + 2 * i) if i % 2 == 0 else (1_000 + 2 * i)   # packed range, below it
+        reqs.append(sv.Request(i, gf.Job.prefix(b, 9, 2 * B), 0.001 * i))
+    srv = sv.Server(B=B, budget_bytes=10**9, capacity=lambda n: 2, validate_group=2, keep_digits=True)
+    comps = srv.run(reqs, timeout_s=300)
+    assert sorted(c.id for c in comps) == list(range(8))
+    for r, c in zip(reqs, comps):
+        assert c.gl_ok and np.array_equal(c.digits, _oracle_prefix(oracle, r.job, B))
+    # which pools served which bases: packed-only pools never took a small base
+    by_pool = {}
+    for c in comps:
+        by_pool.setdefault(c.pool, set()).add(sv._packed_pool(c.b, 9))
+    assert any(kinds == {True} for kinds in by_pool.values())
