@@ -143,21 +143,20 @@ __device__ __forceinline__ bool absorb(int32_t (&dg)[D], int64_t c, const CarryK
 }
 
 // Carry into segment s (16 digits) of a register with N / SEG segments.
-// Takes the pending carry into segment s (negated across the wrap) and clears
-// it, so that a carry is absorbed exactly once even when the test sits out
-// later squarings of its batch (DUP_BITS, position below 0) while batch-wide
-// fix-ups keep running.
-__device__ __forceinline__ int64_t take_carry(const TestDesc &d, size_t s, size_t nseg)
+// Takes the pending carry into segment s (negated across the wrap).  With
+// `clear` it is also cleared, so that a test which sits out later squarings of
+// its batch (DUP_BITS, position below 0) never has it applied twice: needed
+// where nothing overwrites the carries after the absorption (the stand-alone
+// fix-ups, a forward transform of a multiplicand, a cluster loading a test);
+// a squaring or product rewrites every carry of every test it absorbs for.
+__device__ __forceinline__ int64_t take_carry(const TestDesc &d, size_t s, size_t nseg, bool clear = true)
 {
 	int64_t *const p = (s == 0) ? &d.carry[nseg - 1] : &d.carry[s - 1];
 	const int64_t c = *p;
-	if (c != 0) *p = 0;
+	if (clear && (c != 0)) *p = 0;
 	return (s == 0) ? -c : c;
 }
 
-// Absorbs the pending carry of one segment held in shared memory (element i
-// of the segment at seg[i * istride]) and writes the touched digits back to
-// the register in global memory at g.
 __device__ __forceinline__ void fix_segment(const TestDesc &d, int32_t *seg, int istride, int32_t *g, int64_t cin,
 											uint32_t *err)
 {
@@ -698,7 +697,7 @@ __device__ __forceinline__ void col_fwd_body(const Args &a, const TestDesc &d, u
 		{
 			const int k = e / (S::CW / SEG), sg = e % (S::CW / SEG);
 			const size_t j0 = static_cast<size_t>(k) * C + c0 + sg * SEG;
-			fix_segment(d, dg + MP::addr(k, sg * SEG), 1, srcreg + j0, take_carry(d, j0 / SEG, nseg), a.err);
+			fix_segment(d, dg + MP::addr(k, sg * SEG), 1, srcreg + j0, take_carry(d, j0 / SEG, nseg, a.op == OP_FWD), a.err);
 		}
 		__syncthreads();
 		for (int e = threadIdx.x; e < S::R * S::CW; e += blockDim.x)
@@ -963,7 +962,7 @@ __device__ __forceinline__ void col_fwd_reg_body(const Args &a, const TestDesc &
 		{
 			const int k = e / (T / SEG), s = e % (T / SEG);
 			const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
-			fix_segment(d, sm + k * (T + 1) + s * SEG, 1, srcreg + j0, take_carry(d, j0 / SEG, nseg), a.err);
+			fix_segment(d, sm + k * (T + 1) + s * SEG, 1, srcreg + j0, take_carry(d, j0 / SEG, nseg, a.op == OP_FWD), a.err);
 		}
 		__syncthreads();
 #pragma unroll
@@ -1071,7 +1070,8 @@ constexpr int PCOL_THREADS = 256;
 
 // Takes (and clears) the packed carry into segment s: the previous
 // segment's, negated across the wrap (b^N = -1).
-__device__ __forceinline__ void take_carry5(const TestDesc &d, size_t s, size_t nseg, int64_t (&c)[PK_CARRY])
+__device__ __forceinline__ void take_carry5(const TestDesc &d, size_t s, size_t nseg, int64_t (&c)[PK_CARRY],
+											bool clear = true)
 {
 	const size_t src = (s == 0) ? nseg - 1 : s - 1;
 	int64_t *const p = d.carry + PK_CARRY * src;
@@ -1079,26 +1079,27 @@ __device__ __forceinline__ void take_carry5(const TestDesc &d, size_t s, size_t 
 	for (int k = 0; k < PK_CARRY; ++k)
 	{
 		const int64_t v = p[k];
-		if (v != 0) p[k] = 0;
+		if (clear && (v != 0)) p[k] = 0;
 		c[k] = (s == 0) ? -v : v;
 	}
 }
 
 __device__ __forceinline__ void fix_segment5(const TestDesc &d, int32_t *seg, int32_t *g, size_t s, size_t nseg,
-											 uint32_t *err)
+											 bool clear, uint32_t *err)
 {
 	int64_t c[PK_CARRY];
-	take_carry5(d, s, nseg, c);
+	take_carry5(d, s, nseg, c, clear);
 	bool any = false;
 #pragma unroll
 	for (int k = 0; k < PK_CARRY; ++k) any |= (c[k] != 0);
 	if (!any) return;
-	int32_t dg[SEG];
+	int32_t dg[SEG], old[SEG];
 #pragma unroll
-	for (int i = 0; i < SEG; ++i) dg[i] = seg[i];
+	for (int i = 0; i < SEG; ++i) old[i] = dg[i] = seg[i];
 	if (!absorb5<SEG>(dg, c, d.ck)) atomicOr(err, 1u);
 #pragma unroll
-	for (int i = 0; i < SEG; ++i) { seg[i] = dg[i]; g[i] = dg[i]; }
+	for (int i = 0; i < SEG; ++i)
+		if (dg[i] != old[i]) { seg[i] = dg[i]; g[i] = dg[i]; }     // write back the digits that changed
 }
 
 // Digits -> packed residues -> first LR forward stages (one packed column per
@@ -1129,7 +1130,7 @@ __device__ __forceinline__ void pcol_fwd_body(const Args &a, const TestDesc &d, 
 		{
 			const int k = e / (2 * T / SEG), s = e % (2 * T / SEG);
 			const size_t j0 = 2 * (static_cast<size_t>(k) * Cp + c0) + static_cast<size_t>(s) * SEG;
-			fix_segment5(d, sm + k * RW + s * SEG, srcreg + j0, j0 / SEG, nseg, a.err);
+			fix_segment5(d, sm + k * RW + s * SEG, srcreg + j0, j0 / SEG, nseg, a.op == OP_FWD, a.err);
 		}
 		__syncthreads();
 #pragma unroll
