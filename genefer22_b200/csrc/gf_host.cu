@@ -972,8 +972,9 @@ void check_digits(const gfc_batch &bt, size_t test, const int32_t *in)
 
 gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_regs, int device, void *stream)
 {
-	if ((b == nullptr) || (count == 0) || (n < 10) || (n > 23) || (num_regs < 1) || (num_regs > 1024))
-		fail(GFC_ERR_ARG, "gfc_create: need b, count >= 1, 10 <= n <= 23, 1 <= num_regs <= 1024");
+	// the kernels put the test index on grid.y (at most 65535)
+	if ((b == nullptr) || (count == 0) || (count > 65535) || (n < 10) || (n > 23) || (num_regs < 1) || (num_regs > 1024))
+		fail(GFC_ERR_ARG, "gfc_create: need b, 1 <= count <= 65535, 10 <= n <= 23, 1 <= num_regs <= 1024");
 	std::unique_ptr<gfc_batch> bt(new gfc_batch());
 	bt->device = device; bt->n = static_cast<int>(n); bt->N = size_t(1) << n; bt->count = count; bt->num_regs = num_regs;
 	bt->b.assign(b, b + count);

@@ -116,7 +116,7 @@ int gfc_sync(gfc_transform *t);
 
 /* ------------------------------------------------------------------ batches of tests */
 
-/* count tests of the same n with bases b[0..count-1] (each test picks its own
+/* count (1 <= count <= 65535) tests of the same n with bases b[0..count-1] (each test picks its own
  * RNS width), num_regs registers each. */
 int gfc_batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_regs, int device, void *stream,
 					 gfc_batch **out);

@@ -41,6 +41,17 @@ def test_create_without_gpu_fails_cleanly():
         Transform(1000, 12)
 
 
+def test_batch_arguments_checked_before_device_work():
+    """Out-of-range batch arguments fail with GFC_ERR_ARG before any CUDA
+    call, so this runs without a GPU."""
+    from genefer22_b200 import GfcError
+    from genefer22_b200.transform import Batch
+    for bases, n, regs in (([1000] * 65536, 12, 3), ([1000], 9, 3), ([1000], 24, 3), ([1000], 12, 0)):
+        with pytest.raises(GfcError) as e:
+            Batch(bases, n, regs)
+        assert e.value.code == -1, e.value
+
+
 def test_gint_matches_oracle(oracle):
     rng = np.random.default_rng(3)
     for b in (1024, 65538, 2 * 10**9 - 2):
