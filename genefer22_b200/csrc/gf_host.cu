@@ -443,14 +443,27 @@ void mid_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep, int p
 	after_launch();
 }
 
+// The middle pass in registers (k_midr): one thread per column of each plane.
+template <int LR2>
+void midr_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
+{
+	if (prep) return;
+	const size_t C = size_t(1) << (a.n - MID_LR1 - LR2);
+	const dim3 grid(static_cast<unsigned>((size_t(1) << MID_LR1) * size_t(planes) * (C / MIDR_THREADS)),
+					static_cast<unsigned>(grid_y));
+	if (inv) k_midr<LR2, true><<<grid, MIDR_THREADS, 0, s>>>(a);
+	else k_midr<LR2, false><<<grid, MIDR_THREADS, 0, s>>>(a);
+	after_launch();
+}
+
 void launch_mid(int lr2, bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep, int planes = 3)
 {
 	switch (lr2)
 	{
-		case 3: mid_t<3>(inv, a, grid_y, s, prep, planes); break;
-		case 4: mid_t<4>(inv, a, grid_y, s, prep, planes); break;
-		case 5: mid_t<5>(inv, a, grid_y, s, prep, planes); break;
-		case 6: mid_t<6>(inv, a, grid_y, s, prep, planes); break;
+		case 3: midr_t<3>(inv, a, grid_y, s, prep, planes); break;
+		case 4: midr_t<4>(inv, a, grid_y, s, prep, planes); break;
+		case 5: midr_t<5>(inv, a, grid_y, s, prep, planes); break;
+		case 6: midr_t<6>(inv, a, grid_y, s, prep, planes); break;
 		case 7: mid_t<7>(inv, a, grid_y, s, prep, planes); break;
 		default: fail(GFC_ERR_ARG, "six-step plan needs 3 <= lr2 <= 7");
 	}
@@ -485,26 +498,40 @@ bool plan_valid(int n, int lr)
 	return (lr >= 3) && (lr <= 10) && (lc >= 8) && (lc <= 13) && ((lr <= 4) || (col_width(lr) <= (1 << lc)));
 }
 
-// Default plan code: single-CTA up to n = 14, four-step with rows of 2^12
-// (fewer below n = 15), six-step with rows of 2^12 from n = 21, where a
-// 2^(n-12)-point column tile would leave one or two CTAs per SM.
-// Default plan of a batch of at least 2^21 digits whose bases all fit packed
-// digits (n >= 17):
-// four-step on N/2 with 16-row columns up to n = 18, six-step on N/2 above
-// (measured fastest per n on one B200).
-int default_packed_plan(int n)
-{
-	if (n <= 18) return PLAN_PACKED + 4;
-	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 4, 6, 6 };
-	return PLAN_PACKED_SIX + lr2[n];
-}
-
+// Default plans, the fastest per n measured on one B200 (graph replay of each
+// candidate).  Without packed digits (single tests of 2 and 3 primes):
+// single-CTA up to n = 14, four-step with rows of 2^12 at n = 15, 16, then
+// six-step (16-point register column pass, register middle pass of 2^lr2
+// points) with lr2 = 3 for n = 17..19, 5 for n = 20, 21, 6 for n = 22 and 7 for
+// n = 23.
 int default_plan(int n)
 {
 	if (n <= SMALL_MAX_LOGN) return 0;
-	if (n >= 21) return PLAN_SIX + (n - MID_LR1 - 12);
-	const int lc = (n - 3 < 12) ? n - 3 : 12;
-	return n - lc;
+	if (n <= 16) return n - 12;
+	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 3, 5, 5, 6, 7 };
+	return PLAN_SIX + lr2[n];
+}
+
+// Packed digits halve the transform's length, so below n = 20 they pay only
+// with enough tests in the batch to fill the GPU: the default packs a batch of
+// at least this many tests whose bases all fit (0: never).
+size_t packed_min_tests(int n)
+{
+	if (n <= 15) return 0;
+	static const size_t m[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 8, 1, 4, 2, 1, 1, 1, 1 };
+	return m[n];
+}
+
+// Default packed plan: four-step on N/2 with 8-row columns at n = 16 and at
+// n = 17 below 2^21 digits, 16-row columns at n = 17 (2^21 digits and more)
+// and n = 18; six-step on N/2 above.
+int default_packed_plan(int n, size_t count)
+{
+	if (n == 16) return PLAN_PACKED + 3;
+	if (n == 17) return PLAN_PACKED + (((count << 17) >= (size_t(1) << 21)) ? 4 : 3);
+	if (n == 18) return PLAN_PACKED + 4;
+	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 5, 5, 6 };
+	return PLAN_PACKED_SIX + lr2[n];
 }
 
 }  // namespace
@@ -614,9 +641,9 @@ void apply_plan(gfc_batch &bt, int code)
 	}
 	else if (code == PLAN_CLUSTER)
 	{
-		// products keep the default four-step plan of 15 <= n <= 17
+		// products keep the default plan of 15 <= n <= 17
+		apply_plan(bt, default_plan(bt.n));
 		bt.cluster = bt.n - ClusterShape<2>::LC;
-		bt.lr = default_plan(bt.n);
 	}
 	else if (code > PLAN_SIX)
 	{
@@ -1036,14 +1063,13 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 	std::vector<int64_t> pos(count, -1);
 	GFC_CK(cudaMemcpyAsync(bt->d_pos, pos.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, bt->stream));
 	GFC_CK(cudaStreamSynchronize(bt->stream));
-	// packed digits halve the transform's parallelism: the default for batches
-	// of at least 2^21 digits (measured crossover at n = 17 .. 21)
-	bool packable = (bt->n >= 17) && ((size_t(count) << bt->n) >= (size_t(1) << 21));
+	const size_t pmin = packed_min_tests(bt->n);
+	bool packable = (pmin > 0) && (count >= pmin);
 	for (size_t i = 0; packable && (i < count); ++i) packable = packed_ok(b[i], bt->n);
 	if (packable)
 	{
 		set_packed(*bt, true);
-		apply_plan(*bt, default_packed_plan(bt->n));
+		apply_plan(*bt, default_packed_plan(bt->n, count));
 	}
 	prepare_plan(*bt);
 	return bt.release();

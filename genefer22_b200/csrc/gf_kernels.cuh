@@ -868,6 +868,76 @@ __global__ void __launch_bounds__(col_threads(LR)) k_col_inv(const Args a)
 	if (d.set == 0) col_inv_body<0, LR>(a, d, dup, sm); else col_inv_body<1, LR>(a, d, dup, sm);
 }
 
+// ---- transforms of one thread's registers.
+//
+// A whole 2^L-point transform (base `base`, stages 0 .. L-1 of it) on an
+// array the thread owns, in the passes of Sched<L>: pass p covers the stages
+// 4p .. 4p + r - 1 as groups of 2^r elements with stride 2^sh, sh = L - 4p - r;
+// the groups of sub-block blk share the roots tw[(((base << 4p) + blk) << t) + sb],
+// loaded once per sub-block.  The same butterflies in the same order as
+// pass_all over a tile, so the results are identical.  base >= 2 (no
+// normalisation: never the first stage of a whole transform).
+template <class Z, int L>
+__device__ __forceinline__ void fwd_thread(const Z &z, uint32_t (&x)[1 << L], uint32_t base, const uint32_t *__restrict__ tw)
+{
+	if constexpr (L <= 4) { fwd_reg<Z, L>(z, x, base, tw); return; }
+	static_for<0, Sched<L>::NP>([&](auto P) {
+		constexpr int p = decltype(P)::value, s0 = 4 * p, r = Sched<L>::r(p), sh = L - s0 - r;
+#pragma unroll
+		for (int blk = 0; blk < (1 << s0); ++blk)
+		{
+			uint32_t w[(1 << r) - 1];
+			load_twiddles<r>(w, (base << s0) + static_cast<uint32_t>(blk), tw);
+#pragma unroll
+			for (int t = 0; t < r; ++t)
+			{
+				const int half = 1 << (r - 1 - t);
+#pragma unroll
+				for (int sb = 0; sb < (1 << t); ++sb)
+#pragma unroll
+					for (int mm = 0; mm < half; ++mm)
+#pragma unroll
+						for (int o = 0; o < (1 << sh); ++o)
+						{
+							const int i0 = (blk << (L - s0)) + o + ((sb * 2 * half + mm) << sh);
+							bfly_ct(z, x[i0], x[i0 + (half << sh)], w[(1 << t) - 1 + sb]);
+						}
+			}
+		}
+	});
+}
+
+template <class Z, int L>
+__device__ __forceinline__ void inv_thread(const Z &z, uint32_t (&x)[1 << L], uint32_t base, const uint32_t *__restrict__ twi)
+{
+	if constexpr (L <= 4) { inv_reg<Z, L>(z, x, base, twi, false, 0u, 0u); return; }
+	constexpr int NP = Sched<L>::NP;
+	static_for<0, NP>([&](auto Q) {
+		constexpr int p = NP - 1 - decltype(Q)::value, s0 = 4 * p, r = Sched<L>::r(p), sh = L - s0 - r;
+#pragma unroll
+		for (int blk = 0; blk < (1 << s0); ++blk)
+		{
+			uint32_t w[(1 << r) - 1];
+			load_twiddles<r>(w, (base << s0) + static_cast<uint32_t>(blk), twi);
+#pragma unroll
+			for (int t = r - 1; t >= 0; --t)
+			{
+				const int half = 1 << (r - 1 - t);
+#pragma unroll
+				for (int sb = 0; sb < (1 << t); ++sb)
+#pragma unroll
+					for (int mm = 0; mm < half; ++mm)
+#pragma unroll
+						for (int o = 0; o < (1 << sh); ++o)
+						{
+							const int i0 = (blk << (L - s0)) + o + ((sb * 2 * half + mm) << sh);
+							bfly_gs(z, x[i0], x[i0 + (half << sh)], w[(1 << t) - 1 + sb]);
+						}
+			}
+		}
+	});
+}
+
 // ---- six-step middle pass.
 //
 // With R = R1 R2 rows (R1 = 2^MID_LR1), the column transform of length R is
@@ -931,6 +1001,52 @@ __global__ void __launch_bounds__(col_threads(LR2)) k_mid(const Args a)
 	if (d.set == 0) mid_body<0, LR2, INV>(a, d, sm);
 	else if (d.set == 1) mid_body<1, LR2, INV>(a, d, sm);
 	else mid_body<2, LR2, INV>(a, d, sm);
+}
+
+// The middle pass in registers: a thread owns one column of one plane of one
+// block of 2^LR2 rows (2^LR2 words at stride C, a warp's 32 consecutive columns
+// making each load and store one 128-byte line), so the pass needs no shared
+// memory and no barrier.  blockIdx.x = (m P + plane) (C / MIDR_THREADS) + chunk
+// of MIDR_THREADS columns, P = planes of the launch; a CTA whose plane the test
+// does not have returns.
+constexpr int MIDR_THREADS = 128;
+constexpr int MIDR_LOG = 7;
+
+template <int SET, int LR2, bool INV>
+__device__ __forceinline__ void midr_body(const Args &a, const TestDesc &d, int m, int pl, size_t c)
+{
+	if (pl >= PrimeSet<SET>::W) return;
+	const int lc = a.n - MID_LR1 - LR2;
+	const size_t N = size_t(1) << a.n, C = size_t(1) << lc;
+	uint32_t *p = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(pl) * N +
+				  ((static_cast<size_t>(m) << LR2) << lc) + c;
+	const auto z = prime_rt<SET>(pl);
+	uint32_t x[1 << LR2];
+#pragma unroll
+	for (int k = 0; k < (1 << LR2); ++k) x[k] = p[k * C];
+	const uint32_t base = (1u << MID_LR1) + static_cast<uint32_t>(m);
+	if constexpr (INV) inv_thread<decltype(z), LR2>(z, x, base, a.tab[SET].iv[pl]);
+	else fwd_thread<decltype(z), LR2>(z, x, base, a.tab[SET].fw[pl]);
+#pragma unroll
+	for (int k = 0; k < (1 << LR2); ++k) p[k * C] = x[k];
+}
+
+template <int LR2, bool INV>
+__global__ void __launch_bounds__(MIDR_THREADS) k_midr(const Args a)
+{
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	const int chunks_log = a.n - MID_LR1 - LR2 - MIDR_LOG;
+	const int P = static_cast<int>(gridDim.x >> (MID_LR1 + chunks_log));
+	const int q = static_cast<int>(blockIdx.x >> chunks_log);
+	const int m = q / P, pl = q % P;
+	const size_t c = (static_cast<size_t>(blockIdx.x & ((1u << chunks_log) - 1)) << MIDR_LOG) + threadIdx.x;
+	if (d.set == 0) midr_body<0, LR2, INV>(a, d, m, pl, c);
+	else if (d.set == 1) midr_body<1, LR2, INV>(a, d, m, pl, c);
+	else midr_body<2, LR2, INV>(a, d, m, pl, c);
 }
 
 // ---- four-step with R <= 16 rows: one thread owns a whole column.

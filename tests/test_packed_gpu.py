@@ -55,8 +55,8 @@ def test_packed_vs_oracle(oracle, n, plan, b):
     assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), "mul 2"
 
 
-@pytest.mark.parametrize("n,plan,b", [(18, 304, 100_000_002), (20, 305, 50_000_000), (22, 305, 35_000_000),
-                                      (23, 306, 25_000_002)])
+@pytest.mark.parametrize("n,plan,b", [(17, 303, 150_000_000), (18, 304, 100_000_002), (20, 305, 50_000_000),
+                                      (21, 307, 77_000_000), (22, 305, 35_000_000), (23, 306, 25_000_002)])
 def test_packed_six_step_vs_oracle(oracle, n, plan, b):
     """Packed digits with the six-step split of the half-length transform."""
     rng = np.random.default_rng(n + 7)
