@@ -323,9 +323,9 @@ struct PackK
 	uint32_t bm[4];             // b mod p_k in Montgomery form (packing d0 + b d1)
 };
 
-// Adds the CRT value of one packed coefficient (residues x[4]) times f to the
-// window at positions 0..6.
-__device__ __forceinline__ void crt_window(const uint32_t x[4], int dup, const CarryK &K, const PackK &P, int64_t (&win)[7])
+// Garner's mixed-radix digits a1..a4 of one packed coefficient (residues
+// x[4]), a4 carrying in bit 31 the flag V > M/2 (a4 < p4 < 2^31).
+__device__ __forceinline__ void crt_garner4(uint32_t (&x)[4])
 {
 	using C = Crt<2>;
 	using Z2 = Zp<C::p2, true>;
@@ -345,9 +345,16 @@ __device__ __forceinline__ void crt_window(const uint32_t x[4], int dup, const C
 	const uint64_t low = static_cast<uint64_t>(a2) * C::p1 + a1;            // < p1 p2
 	const bool rest_hi = (a3 > (C::p3 - 1) / 2) || ((a3 == (C::p3 - 1) / 2) && (low > P12 / 2));
 	const bool z = (a4 > (C::p4 - 1) / 2) || ((a4 == (C::p4 - 1) / 2) && rest_hi);
+	x[0] = a1; x[1] = a2; x[2] = a3; x[3] = a4 | (z ? 0x80000000u : 0u);
+}
+
+// Adds f V (mixed-radix digits g from crt_garner4) to the window at
+// positions 0..6.
+__device__ __forceinline__ void crt_window_g(const uint32_t (&g)[4], int dup, const PackK &P, int64_t (&win)[7])
+{
 	const int f = dup;                                                       // index f - 1
-	const int64_t zm = z ? 1 : 0;
-	const uint64_t A1 = a1, A2 = a2, A3 = a3, A4 = a4;
+	const int64_t zm = static_cast<int64_t>(g[3] >> 31);
+	const uint64_t A1 = g[0], A2 = g[1], A3 = g[2], A4 = g[3] & 0x7fffffffu;
 	int64_t U[PK_LIMBS];
 	U[0] = static_cast<int64_t>((A1 << dup) + A2 * P.w1[f][0] + A3 * P.w2[f][0] + A4 * P.w3[f][0]) - zm * P.m[f][0];
 	U[1] = static_cast<int64_t>(A2 * P.w1[f][1] + A3 * P.w2[f][1] + A4 * P.w3[f][1]) - zm * P.m[f][1];
@@ -358,6 +365,15 @@ __device__ __forceinline__ void crt_window(const uint32_t x[4], int dup, const C
 	U[6] = -zm * P.m[f][6];
 #pragma unroll
 	for (int j = 0; j < PK_LIMBS; ++j) win[j] += U[j];
+}
+
+// Adds the CRT value of one packed coefficient (residues x[4]) times f to the
+// window at positions 0..6.
+__device__ __forceinline__ void crt_window(const uint32_t x[4], int dup, const PackK &P, int64_t (&win)[7])
+{
+	uint32_t g[4] = { x[0], x[1], x[2], x[3] };
+	crt_garner4(g);
+	crt_window_g(g, dup, P, win);
 }
 
 // Completes the digit at window position 0 and shifts the window by one.

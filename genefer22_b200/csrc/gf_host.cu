@@ -290,6 +290,32 @@ void small_set(int logn, const Args &a, int grid, cudaStream_t s, bool prep)
 	}
 }
 
+// Streaming multiprocessors of the current device (cached per device).
+int sm_count()
+{
+	static std::atomic<int> cache[64];
+	int dev = 0;
+	GFC_CK(cudaGetDevice(&dev));
+	if ((dev < 0) || (dev >= 64)) return 148;
+	int v = cache[dev].load();
+	if (v == 0)
+	{
+		GFC_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+		cache[dev].store(v);
+	}
+	return v;
+}
+
+// A register column launch whose one-thread-per-column grid (256 columns and
+// 8 warps per CTA) holds fewer than `per_sm` warps per SM takes the
+// plane-split kernels instead: a thread per (plane, column).  Measured on one
+// B200: the packed kernels gain below a full SM (32 warps); the unpacked ones,
+// whose CRT phase keeps one thread per segment, only below 8 warps per SM.
+bool split_cols(size_t cols, int grid_y, int per_sm)
+{
+	return (cols / 256) * static_cast<size_t>(grid_y) * 8 < static_cast<size_t>(sm_count()) * static_cast<size_t>(per_sm);
+}
+
 template <int LR>
 void col_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 {
@@ -298,7 +324,16 @@ void col_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 		// R <= 16: a thread owns a column (register kernels)
 		using S = ColRegShape<LR>;
 		if (prep) { set_smem(k_colr_inv<LR>, S::SMEM); return; }
-		const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / COLR_THREADS), static_cast<unsigned>(grid_y));
+		const size_t cols = size_t(1) << (a.n - LR);
+		if (split_cols(cols, grid_y, 8))
+		{
+			const dim3 grid(static_cast<unsigned>(cols / CS_T), static_cast<unsigned>(grid_y));
+			if (inv) k_colr_inv_s<LR><<<grid, WMAX * CS_T, 0, s>>>(a);
+			else k_colr_fwd_s<LR><<<grid, WMAX * CS_T, 0, s>>>(a);
+			after_launch();
+			return;
+		}
+		const dim3 grid(static_cast<unsigned>(cols / COLR_THREADS), static_cast<unsigned>(grid_y));
 		if (inv) k_colr_inv<LR><<<grid, COLR_THREADS, S::SMEM, s>>>(a);
 		else k_colr_fwd<LR><<<grid, COLR_THREADS, 0, s>>>(a);
 		after_launch();
@@ -363,7 +398,16 @@ void pcol_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 {
 	using S = PColShape<LR>;
 	if (prep) { set_smem(k_pcol_inv<LR>, S::SMEM); return; }
-	const dim3 grid(static_cast<unsigned>((size_t(1) << (a.n - LR)) / PCOL_THREADS), static_cast<unsigned>(grid_y));
+	const size_t cols = size_t(1) << (a.n - LR);
+	if (split_cols(cols, grid_y, 32))
+	{
+		const dim3 grid(static_cast<unsigned>(cols / PCS_T), static_cast<unsigned>(grid_y));
+		if (inv) k_pcol_inv_s<LR><<<grid, 4 * PCS_T, 0, s>>>(a);
+		else k_pcol_fwd_s<LR><<<grid, 4 * PCS_T, 0, s>>>(a);
+		after_launch();
+		return;
+	}
+	const dim3 grid(static_cast<unsigned>(cols / PCOL_THREADS), static_cast<unsigned>(grid_y));
 	if (inv) k_pcol_inv<LR><<<grid, PCOL_THREADS, S::SMEM, s>>>(a);
 	else k_pcol_fwd<LR><<<grid, PCOL_THREADS, 0, s>>>(a);
 	after_launch();
@@ -512,24 +556,20 @@ int default_plan(int n)
 	return PLAN_SIX + lr2[n];
 }
 
-// Packed digits halve the transform's length, so below n = 20 they pay only
-// with enough tests in the batch to fill the GPU: the default packs a batch of
-// at least this many tests whose bases all fit (0: never).
+// The default packs a batch of at least this many tests whose bases all fit
+// (0: never): packed digits are faster from one test at n >= 16 (measured on
+// one B200 against the fastest unpacked plan).
 size_t packed_min_tests(int n)
 {
-	if (n <= 15) return 0;
-	static const size_t m[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 8, 1, 4, 2, 1, 1, 1, 1 };
-	return m[n];
+	return (n >= 16) ? 1 : 0;
 }
 
-// Default packed plan: four-step on N/2 with 8-row columns at n = 16 and at
-// n = 17 below 2^21 digits, 16-row columns at n = 17 (2^21 digits and more)
-// and n = 18; six-step on N/2 above.
-int default_packed_plan(int n, size_t count)
+// Default packed plan: four-step on N/2 with 8-row columns at n = 16 and
+// 16-row columns at n = 17, 18; six-step on N/2 above.
+int default_packed_plan(int n)
 {
 	if (n == 16) return PLAN_PACKED + 3;
-	if (n == 17) return PLAN_PACKED + (((count << 17) >= (size_t(1) << 21)) ? 4 : 3);
-	if (n == 18) return PLAN_PACKED + 4;
+	if (n <= 18) return PLAN_PACKED + 4;
 	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 5, 5, 6 };
 	return PLAN_PACKED_SIX + lr2[n];
 }
@@ -1069,7 +1109,7 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 	if (packable)
 	{
 		set_packed(*bt, true);
-		apply_plan(*bt, default_packed_plan(bt->n, count));
+		apply_plan(*bt, default_packed_plan(bt->n));
 	}
 	prepare_plan(*bt);
 	return bt.release();

@@ -1069,20 +1069,24 @@ __device__ __forceinline__ void col_fwd_reg_body(const Args &a, const TestDesc &
 	for (int k = 0; k < R; ++k) dv[k] = src[k * C];
 	if (a.fix)
 	{
-		// pending carries: stage the tile [R][T], one thread per 16-digit segment
+		// pending carries: stage the tile [R][T] (digit c of row k at k RW +
+		// c + c / 16, so that the threads' 16-digit segments start in distinct
+		// banks), one thread per segment
+		constexpr int RW = T + T / SEG;
 #pragma unroll
-		for (int k = 0; k < R; ++k) sm[k * (T + 1) + tid] = dv[k];
+		for (int k = 0; k < R; ++k) sm[k * RW + tid + tid / SEG] = dv[k];
 		__syncthreads();
 		const size_t nseg = N / SEG;
 		for (int e = tid; e < R * (T / SEG); e += T)
 		{
 			const int k = e / (T / SEG), s = e % (T / SEG);
 			const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
-			fix_segment(d, sm + k * (T + 1) + s * SEG, 1, srcreg + j0, take_carry(d, j0 / SEG, nseg, a.op == OP_FWD), a.err);
+			fix_segment(d, sm + k * RW + s * (SEG + 1), 1, srcreg + j0, take_carry(d, j0 / SEG, nseg, a.op == OP_FWD),
+						a.err);
 		}
 		__syncthreads();
 #pragma unroll
-		for (int k = 0; k < R; ++k) dv[k] = sm[k * (T + 1) + tid];
+		for (int k = 0; k < R; ++k) dv[k] = sm[k * RW + tid + tid / SEG];
 	}
 	for_planes<SET>([&](auto PLc) {
 		constexpr int PL = decltype(PLc)::value;
@@ -1143,11 +1147,11 @@ __device__ __forceinline__ void col_inv_reg_body(const Args &a, const TestDesc &
 	}
 }
 
-// Shared memory: [R][T + 1] int32 staging of the digits when fixing carries.
+// Shared memory: [R][T + T/16] int32 staging of the digits when fixing carries.
 template <int LR>
 __global__ void __launch_bounds__(COLR_THREADS) k_colr_fwd(const Args a)
 {
-	__shared__ int32_t sm[(1 << LR) * (COLR_THREADS + 1)];
+	__shared__ int32_t sm[(1 << LR) * (COLR_THREADS + COLR_THREADS / SEG)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
 	bool active;
@@ -1172,6 +1176,120 @@ __global__ void __launch_bounds__(COLR_THREADS) k_colr_inv(const Args a)
 	const bool dup = get_dup(a, d, t, a.j, active);
 	if (!active) return;
 	if (d.set == 0) col_inv_reg_body<0, LR>(a, d, dup, sm); else col_inv_reg_body<1, LR>(a, d, dup, sm);
+}
+
+// ---- plane-split register columns, for batches too small to fill the GPU
+// with one thread per column: a CTA takes CS_T columns and has a thread per
+// (plane, column), WMAX planes (threads of planes the test does not have only
+// join the barriers).  Same arithmetic in the same order as the kernels above.
+
+constexpr int CS_T = 64;
+
+template <int SET, int LR>
+__device__ __forceinline__ void col_fwd_split_body(const Args &a, const TestDesc &d, int32_t *sm)
+{
+	constexpr int R = 1 << LR, T = CS_T, NT = WMAX * T, RW = T + T / SEG;
+	const size_t N = size_t(1) << a.n, C = size_t(1) << (a.n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x, c = tid % T, pl = tid / T;
+	int32_t *const srcreg = d.regs + static_cast<size_t>(a.src) * N;
+	if (a.fix)
+	{
+		// the tile [R][T], digit c of row k at k RW + c + c / 16; one thread per segment
+		for (int e = tid; e < R * T; e += NT)
+		{
+			const int k = e / T, cc = e % T;
+			sm[k * RW + cc + cc / SEG] = srcreg[static_cast<size_t>(k) * C + c0 + cc];
+		}
+		__syncthreads();
+		const size_t nseg = N / SEG;
+		for (int e = tid; e < R * (T / SEG); e += NT)
+		{
+			const int k = e / (T / SEG), s = e % (T / SEG);
+			const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
+			fix_segment(d, sm + k * RW + s * (SEG + 1), 1, srcreg + j0, take_carry(d, j0 / SEG, nseg, a.op == OP_FWD),
+						a.err);
+		}
+		__syncthreads();
+	}
+	if (pl >= PrimeSet<SET>::W) return;
+	const auto z = prime_rt<SET>(pl);
+	uint32_t x[R];
+#pragma unroll
+	for (int k = 0; k < R; ++k)
+		x[k] = z.from_int(a.fix ? sm[k * RW + c + c / SEG] : srcreg[static_cast<size_t>(k) * C + c0 + c]);
+	fwd_reg<decltype(z), LR>(z, x, 1u, a.tab[SET].fw[pl]);
+	uint32_t *dst = ((a.op == OP_FWD) ? d.zp : d.planes) + pl * N + c0 + c;
+#pragma unroll
+	for (int k = 0; k < R; ++k) dst[k * C] = x[k];
+}
+
+template <int SET, int LR>
+__device__ __forceinline__ void col_inv_split_body(const Args &a, const TestDesc &d, bool dup, uint32_t *sm)
+{
+	constexpr int R = 1 << LR, W = PrimeSet<SET>::W;
+	constexpr int T = CS_T, NT = WMAX * T, RS = T + T / 16, PS = R * RS, SPR = T / SEG;
+	const size_t N = size_t(1) << a.n, C = size_t(1) << (a.n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x, c = tid % T, pl = tid / T;
+	using MP = ColMap<RS>;
+	if (pl < W)
+	{
+		const auto z = prime_rt<SET>(pl);
+		const uint32_t *src = d.planes + pl * N + c0 + c;
+		uint32_t x[R];
+#pragma unroll
+		for (int k = 0; k < R; ++k) x[k] = src[k * C];
+		inv_reg<decltype(z), LR>(z, x, 1u, a.tab[SET].iv[pl], true, __ldg(&a.tab[SET].fw[pl][0]),
+								 __ldg(&a.tab[SET].iv[pl][0]));
+#pragma unroll
+		for (int k = 0; k < R; ++k) sm[pl * PS + MP::addr(k, c)] = x[k];
+	}
+	__syncthreads();
+	int32_t *out = d.regs + static_cast<size_t>(a.dst) * N;
+	for (int e = tid; e < R * SPR; e += NT)
+	{
+		const int k = e / SPR, s = e % SPR;
+		const size_t j0 = static_cast<size_t>(k) * C + c0 + s * SEG;
+		int64_t cr = 0;
+		int32_t dg[SEG];
+#pragma unroll
+		for (int i = 0; i < SEG; ++i)
+		{
+			uint32_t x[3];
+#pragma unroll
+			for (int q = 0; q < W; ++q) x[q] = sm[q * PS + MP::addr(k, s * SEG + i)];
+			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, cr);
+		}
+		int4 *o = reinterpret_cast<int4 *>(out + j0);
+#pragma unroll
+		for (int i = 0; i < SEG / 4; ++i) o[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
+		d.carry[j0 / SEG] = cr;
+	}
+}
+
+template <int LR>
+__global__ void __launch_bounds__(WMAX * CS_T) k_colr_fwd_s(const Args a)
+{
+	__shared__ int32_t sm[(1 << LR) * (CS_T + CS_T / SEG)];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) col_fwd_split_body<0, LR>(a, d, sm); else col_fwd_split_body<1, LR>(a, d, sm);
+}
+
+template <int LR>
+__global__ void __launch_bounds__(WMAX * CS_T) k_colr_inv_s(const Args a)
+{
+	__shared__ __align__(16) uint32_t sm[WMAX * (1 << LR) * (CS_T + CS_T / 16)];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	const bool dup = get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	if (d.set == 0) col_inv_split_body<0, LR>(a, d, dup, sm); else col_inv_split_body<1, LR>(a, d, dup, sm);
 }
 
 // ---- packed digits (prime set 2).
@@ -1223,7 +1341,7 @@ __device__ __forceinline__ void fix_segment5(const TestDesc &d, int32_t *seg, in
 template <int LR>
 __device__ __forceinline__ void pcol_fwd_body(const Args &a, const TestDesc &d, int32_t *sm)
 {
-	constexpr int R = 1 << LR, T = PCOL_THREADS, RW = 2 * T + 2;
+	constexpr int R = 1 << LR, T = PCOL_THREADS, RW = 2 * T + 2 * T / SEG;
 	const size_t Np = size_t(1) << a.n, Cp = size_t(1) << (a.n - LR);
 	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
 	const int tid = threadIdx.x;
@@ -1238,19 +1356,22 @@ __device__ __forceinline__ void pcol_fwd_body(const Args &a, const TestDesc &d, 
 	}
 	if (a.fix)
 	{
+		// digit j of row k at k RW + j + j / 16: the threads' 16-digit segments
+		// start in distinct banks
+		const int o = 2 * tid + tid / (SEG / 2);
 #pragma unroll
-		for (int k = 0; k < R; ++k) { sm[k * RW + 2 * tid] = d0[k]; sm[k * RW + 2 * tid + 1] = d1[k]; }
+		for (int k = 0; k < R; ++k) { sm[k * RW + o] = d0[k]; sm[k * RW + o + 1] = d1[k]; }
 		__syncthreads();
 		const size_t nseg = (2 * Np) / SEG;
 		for (int e = tid; e < R * (2 * T / SEG); e += T)
 		{
 			const int k = e / (2 * T / SEG), s = e % (2 * T / SEG);
 			const size_t j0 = 2 * (static_cast<size_t>(k) * Cp + c0) + static_cast<size_t>(s) * SEG;
-			fix_segment5(d, sm + k * RW + s * SEG, srcreg + j0, j0 / SEG, nseg, a.op == OP_FWD, a.err);
+			fix_segment5(d, sm + k * RW + s * (SEG + 1), srcreg + j0, j0 / SEG, nseg, a.op == OP_FWD, a.err);
 		}
 		__syncthreads();
 #pragma unroll
-		for (int k = 0; k < R; ++k) { d0[k] = sm[k * RW + 2 * tid]; d1[k] = sm[k * RW + 2 * tid + 1]; }
+		for (int k = 0; k < R; ++k) { d0[k] = sm[k * RW + o]; d1[k] = sm[k * RW + o + 1]; }
 	}
 	for_planes<2>([&](auto PLc) {
 		constexpr int PL = decltype(PLc)::value;
@@ -1313,7 +1434,7 @@ __device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, 
 			uint32_t x[4];
 #pragma unroll
 			for (int pl = 0; pl < 4; ++pl) x[pl] = sm[pl * PS + S::addr(k, s * (SEG / 2) + ci)];
-			crt_window(x, dup ? 1 : 0, d.ck, d.pk, win);
+			crt_window(x, dup ? 1 : 0, d.pk, win);
 			dg[2 * ci] = window_digit(d.ck, win);
 			dg[2 * ci + 1] = window_digit(d.ck, win);
 		}
@@ -1329,7 +1450,7 @@ __device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, 
 template <int LR>
 __global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_fwd(const Args a)
 {
-	__shared__ int32_t sm[(1 << LR) * (2 * PCOL_THREADS + 2)];
+	__shared__ int32_t sm[(1 << LR) * (2 * PCOL_THREADS + 2 * PCOL_THREADS / SEG)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
 	bool active;
@@ -1348,6 +1469,159 @@ __global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_inv(const Args a)
 	const bool dup = get_dup(a, d, t, a.j, active);
 	if (!active) return;
 	pcol_inv_body<LR>(a, d, dup, sm);
+}
+
+// Plane-split packed columns for batches too small to fill the GPU with one
+// thread per packed column: a CTA takes PCS_T columns with a thread per
+// (plane, column), 4 PCS_T threads.  The inverse kernel then runs Garner's
+// step per coefficient over all threads (digits back into the tile), and the
+// digit window per 8-coefficient segment.
+constexpr int PCS_T = 64;
+
+template <int LR>
+__device__ __forceinline__ void pcol_fwd_split_body(const Args &a, const TestDesc &d, int32_t *sm)
+{
+	constexpr int R = 1 << LR, T = PCS_T, NT = 4 * T, RW = 2 * T + 2 * T / SEG;
+	const size_t Np = size_t(1) << a.n, Cp = size_t(1) << (a.n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x, c = tid % T, pl = tid / T;
+	int32_t *const srcreg = d.regs + static_cast<size_t>(a.src) * (2 * Np);
+	if (a.fix)
+	{
+		// digit j of row k at k RW + j + j / 16; one thread per 16-digit segment
+		for (int e = tid; e < R * T; e += NT)
+		{
+			const int k = e / T, cc = e % T;
+			const int2 v = *reinterpret_cast<const int2 *>(srcreg + 2 * (static_cast<size_t>(k) * Cp + c0 + cc));
+			int32_t *p = sm + k * RW + 2 * cc + cc / (SEG / 2);
+			p[0] = v.x; p[1] = v.y;
+		}
+		__syncthreads();
+		const size_t nseg = (2 * Np) / SEG;
+		for (int e = tid; e < R * (2 * T / SEG); e += NT)
+		{
+			const int k = e / (2 * T / SEG), s = e % (2 * T / SEG);
+			const size_t j0 = 2 * (static_cast<size_t>(k) * Cp + c0) + static_cast<size_t>(s) * SEG;
+			fix_segment5(d, sm + k * RW + s * (SEG + 1), srcreg + j0, j0 / SEG, nseg, a.op == OP_FWD, a.err);
+		}
+		__syncthreads();
+	}
+	const auto z = prime_rt<2>(pl);
+	const uint32_t bm = d.pk.bm[pl];
+	uint32_t x[R];
+#pragma unroll
+	for (int k = 0; k < R; ++k)
+	{
+		int32_t v0, v1;
+		if (a.fix)
+		{
+			const int32_t *p = sm + k * RW + 2 * c + c / (SEG / 2);
+			v0 = p[0]; v1 = p[1];
+		}
+		else
+		{
+			const int2 v = *reinterpret_cast<const int2 *>(srcreg + 2 * (static_cast<size_t>(k) * Cp + c0 + c));
+			v0 = v.x; v1 = v.y;
+		}
+		x[k] = z.add(z.from_int(v0), z.mul(z.from_int(v1), bm));
+	}
+	fwd_reg<decltype(z), LR>(z, x, 1u, a.tab[2].fw[pl]);
+	uint32_t *dst = ((a.op == OP_FWD) ? d.zp : d.planes) + pl * Np + c0 + c;
+#pragma unroll
+	for (int k = 0; k < R; ++k) dst[k * Cp] = x[k];
+}
+
+// Tile of the plane-split inverse: coefficient c of row k at k RS + (c % 8) Q
+// + c / 8 with Q = 12, RS = 104: a warp writing 32 consecutive coefficients of
+// a row, and a warp reading coefficient ci of the 8 segments of 4 rows, both
+// hit 32 distinct banks.
+template <int LR>
+struct PColShapeS
+{
+	static constexpr int R = 1 << LR, T = PCS_T, Q = 12, RS = 8 * Q + 8, PS = R * RS;
+	static constexpr size_t SMEM = size_t(4) * PS * 4;
+	__device__ __forceinline__ static int addr(int k, int c) { return k * RS + (c & 7) * Q + (c >> 3); }
+};
+
+template <int LR>
+__device__ __forceinline__ void pcol_inv_split_body(const Args &a, const TestDesc &d, bool dup, uint32_t *sm)
+{
+	using S = PColShapeS<LR>;
+	constexpr int R = S::R, T = S::T, NT = 4 * T, PS = S::PS, SPR = T / (SEG / 2);
+	const size_t Np = size_t(1) << a.n, Cp = size_t(1) << (a.n - LR);
+	const size_t c0 = static_cast<size_t>(blockIdx.x) * T;
+	const int tid = threadIdx.x;
+	{
+		const int c = tid % T, pl = tid / T;
+		const auto z = prime_rt<2>(pl);
+		const uint32_t *src = d.planes + pl * Np + c0 + c;
+		uint32_t x[R];
+#pragma unroll
+		for (int k = 0; k < R; ++k) x[k] = src[k * Cp];
+		inv_reg<decltype(z), LR>(z, x, 1u, a.tab[2].iv[pl], true, __ldg(&a.tab[2].fw[pl][0]), __ldg(&a.tab[2].iv[pl][0]));
+#pragma unroll
+		for (int k = 0; k < R; ++k) sm[pl * PS + S::addr(k, c)] = x[k];
+	}
+	__syncthreads();
+	for (int e = tid; e < R * T; e += NT)
+	{
+		const int k = e / T, c = e % T;
+		uint32_t g[4];
+#pragma unroll
+		for (int pl = 0; pl < 4; ++pl) g[pl] = sm[pl * PS + S::addr(k, c)];
+		crt_garner4(g);
+#pragma unroll
+		for (int pl = 0; pl < 4; ++pl) sm[pl * PS + S::addr(k, c)] = g[pl];
+	}
+	__syncthreads();
+	int32_t *out = d.regs + static_cast<size_t>(a.dst) * (2 * Np);
+	for (int e = tid; e < R * SPR; e += NT)
+	{
+		const int k = e / SPR, s = e % SPR;
+		const size_t i0 = static_cast<size_t>(k) * Cp + c0 + static_cast<size_t>(s) * (SEG / 2);
+		int64_t win[7] = { 0, 0, 0, 0, 0, 0, 0 };
+		int32_t dg[SEG];
+#pragma unroll
+		for (int ci = 0; ci < SEG / 2; ++ci)
+		{
+			uint32_t g[4];
+#pragma unroll
+			for (int pl = 0; pl < 4; ++pl) g[pl] = sm[pl * PS + S::addr(k, s * (SEG / 2) + ci)];
+			crt_window_g(g, dup ? 1 : 0, d.pk, win);
+			dg[2 * ci] = window_digit(d.ck, win);
+			dg[2 * ci + 1] = window_digit(d.ck, win);
+		}
+		int4 *o = reinterpret_cast<int4 *>(out + 2 * i0);
+#pragma unroll
+		for (int i = 0; i < SEG / 4; ++i) o[i] = make_int4(dg[4 * i], dg[4 * i + 1], dg[4 * i + 2], dg[4 * i + 3]);
+		int64_t *cs = d.carry + PK_CARRY * (i0 / (SEG / 2));
+#pragma unroll
+		for (int q = 0; q < PK_CARRY; ++q) cs[q] = win[q];
+	}
+}
+
+template <int LR>
+__global__ void __launch_bounds__(4 * PCS_T) k_pcol_fwd_s(const Args a)
+{
+	__shared__ int32_t sm[(1 << LR) * (2 * PCS_T + 2 * PCS_T / SEG)];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	pcol_fwd_split_body<LR>(a, d, sm);
+}
+
+template <int LR>
+__global__ void __launch_bounds__(4 * PCS_T) k_pcol_inv_s(const Args a)
+{
+	__shared__ __align__(16) uint32_t sm[4 * PColShapeS<LR>::PS];
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	const bool dup = get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	pcol_inv_split_body<LR>(a, d, dup, sm);
 }
 
 // Pending packed carries of register a.dst absorbed (a.n = n: digits).

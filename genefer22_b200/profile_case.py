@@ -1,6 +1,7 @@
 """A small, fixed squaring case for kernel profiles: one batch of `count`
-tests of size n (bases seeded uniform in [10^6, bmax), even), `squarings`
-squarings of register 0 with the given plan.
+tests of size n (bases seeded uniform in [10^6, bmax), even), register 0 of
+each test loaded with seeded random balanced digits (so that every carry path
+does its full work), then `squarings` squarings with the given plan.
 
     python -m genefer22_b200.profile_case --n 22 --count 1 --squarings 2
 """
@@ -27,7 +28,8 @@ def main():
     with Batch(bases, a.n) as bt:
         if a.plan >= 0:
             bt.set_plan(a.plan)
-        bt.set(3)
+        for i, b in enumerate(bases):
+            bt.put(i, rng.integers(-(b // 2), b // 2, size=1 << a.n, dtype=np.int64).astype(np.int32))
         bt.square(False, a.squarings)
         bt.sync()
         print(f"n={a.n} tests={a.count} plan={bt.plan()} widths={sorted(set(bt.widths().tolist()))} squarings={a.squarings}")

@@ -177,11 +177,10 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
  * base of the batch in the exact range, 2^20 <= b and (N/2)((b/2+1)(b+1))^2
  * below half the primes' product, else GFC_ERR_RANGE; gfc_batch_widths then
  * reports 4); lr = 300 + lr2: packed digits with the six-step split of the
- * half-length transform (8 <= n - 5 - lr2 <= 13).  A new batch uses packed
- * digits when every base is in the packed range and it holds at least 8 tests
- * at n = 16, 1 at n = 17, 4 at n = 18, 2 at n = 19, 1 from n = 20 (203 at
- * n = 16 and 17, 204 at n = 17 from 2^21 digits and at n = 18, 303 at n = 19,
- * 20, 305 at n = 21, 22, 306 at n = 23); otherwise single-CTA up to n = 14,
+ * half-length transform (8 <= n - 5 - lr2 <= 13).  A new batch from n = 16
+ * uses packed digits when every base is in the packed range (203 at n = 16,
+ * 204 at n = 17, 18, 303 at n = 19, 20, 305 at n = 21, 22, 306 at n = 23);
+ * otherwise single-CTA up to n = 14,
  * four-step at n = 15, 16 (lr = n - 12), six-step above (103 at n = 17..19,
  * 105 at n = 20, 21, 106 at n = 22, 107 at n = 23): the fastest plans measured
  * on one B200.

@@ -71,11 +71,15 @@ def test_six_step_plan(oracle, n, plan, b):
 
 
 def test_width_choice():
-    # 2 primes while N (b/2+1)^2 < P1 P2 / 2, else 3
+    # unpacked: 2 primes while N (b/2+1)^2 < P1 P2 / 2, else 3; packed digits
+    # (the default from n = 16 for bases in the packed range): 4
     assert Transform(SMALL_B, 12).width() == 2
     assert Transform(LARGE_B, 12).width() == 3
-    assert Transform(22_000_000, 16).width() == 2
-    assert Transform(23_500_000, 16).width() == 3
+    for b, w in ((22_000_000, 2), (23_500_000, 3)):
+        t = Transform(b, 16)
+        assert t.width() == 4 and t.batch.plan() == 203
+        t.batch.set_plan(4)
+        assert t.width() == w
 
 
 @pytest.mark.parametrize("b", [8, 10, 1024, 1026, 65536 + 2])
