@@ -472,12 +472,12 @@ void launch_cluster_lq(int lq, const Args &a, int ntests, int max_active, cudaSt
 template <int LR2>
 void mid_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 {
-	using S = ColShape<LR2>;
+	using S = MidShape<LR2>;
 	const size_t smem = size_t(planes) * S::PS * 4;
 	if (prep)
 	{
-		set_smem(k_mid<LR2, false>, size_t(4) * S::PS * 4);
-		set_smem(k_mid<LR2, true>, size_t(4) * S::PS * 4);
+		set_smem(k_mid<LR2, false>, S::SMEM);
+		set_smem(k_mid<LR2, true>, S::SMEM);
 		return;
 	}
 	const size_t C = size_t(1) << (a.n - MID_LR1 - LR2);

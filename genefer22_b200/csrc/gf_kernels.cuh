@@ -948,10 +948,30 @@ __device__ __forceinline__ void inv_thread(const Z &z, uint32_t (&x)[1 << L], ui
 // R1 + m.  Tile: R2 rows x CW columns of every plane, planes in and out.
 constexpr int MID_LR1 = 4;
 
+// Unpadded column tile of the middle pass (no CRT reads it): a warp's 32
+// consecutive columns of one row are 32 consecutive words, and the 16-byte
+// staging writes of 8 consecutive threads cover whole rows.
+template <int RS>
+struct ColMapU
+{
+	__device__ __forceinline__ static int addr(int i, int lane) { return i * RS + lane; }
+	__host__ __device__ static constexpr int off(int m, int step) { return m * step * RS; }
+};
+
+template <int LR2>
+struct MidShape
+{
+	static constexpr int R = 1 << LR2;
+	static constexpr int CW = col_width(LR2);
+	static constexpr int CWL = ilog2c(CW);
+	static constexpr int PS = R * CW;                      // plane stride
+	static constexpr size_t SMEM = size_t(4) * PS * 4;     // up to four planes
+};
+
 template <int SET, int LR2, bool INV>
 __device__ __forceinline__ void mid_body(const Args &a, const TestDesc &d, uint32_t *sm)
 {
-	using S = ColShape<LR2>;
+	using S = MidShape<LR2>;
 	constexpr int W = PrimeSet<SET>::W;
 	const int lr = MID_LR1 + LR2, lc = a.n - lr;
 	const size_t N = size_t(1) << a.n, C = size_t(1) << lc;
@@ -961,17 +981,14 @@ __device__ __forceinline__ void mid_body(const Args &a, const TestDesc &d, uint3
 	const size_t row0 = static_cast<size_t>(m) << LR2;
 	// the forward transform of a multiplicand (OP_FWD) lives in zp
 	uint32_t *planes = ((a.op == OP_FWD) ? d.zp : d.planes) + row0 * C + c0;
-	using MP = ColMap<S::RS>;
+	using MP = ColMapU<S::CW>;
 	for (int e = threadIdx.x; e < S::R * S::CW / 4; e += blockDim.x)
 	{
 		const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
 #pragma unroll
 		for (int pl = 0; pl < W; ++pl)
-		{
-			const uint4 u = *reinterpret_cast<const uint4 *>(planes + pl * N + static_cast<size_t>(k) * C + cc);
-			uint32_t *p = sm + pl * S::PS + MP::addr(k, cc);
-			p[0] = u.x; p[1] = u.y; p[2] = u.z; p[3] = u.w;
-		}
+			*reinterpret_cast<uint4 *>(sm + pl * S::PS + MP::addr(k, cc)) =
+				*reinterpret_cast<const uint4 *>(planes + pl * N + static_cast<size_t>(k) * C + cc);
 	}
 	__syncthreads();
 	const uint32_t base = (1u << MID_LR1) + static_cast<uint32_t>(m);
@@ -982,10 +999,8 @@ __device__ __forceinline__ void mid_body(const Args &a, const TestDesc &d, uint3
 		const int k = e >> (S::CWL - 2), cc = (e & (S::CW / 4 - 1)) * 4;
 #pragma unroll
 		for (int pl = 0; pl < W; ++pl)
-		{
-			const uint32_t *p = sm + pl * S::PS + MP::addr(k, cc);
-			*reinterpret_cast<uint4 *>(planes + pl * N + static_cast<size_t>(k) * C + cc) = make_uint4(p[0], p[1], p[2], p[3]);
-		}
+			*reinterpret_cast<uint4 *>(planes + pl * N + static_cast<size_t>(k) * C + cc) =
+				*reinterpret_cast<const uint4 *>(sm + pl * S::PS + MP::addr(k, cc));
 	}
 }
 

@@ -114,13 +114,14 @@ def test_uneven_batch_alone_vs_mix(oracle):
     oracle's for sizes 12 and 13; Gerbicz-Li passes."""
     B = 32
     tests = uneven_tests(count=24, seed=1004)
-    tests += [(2_000_000_000 - 2, 12), (1_000_000_000, 17), (1024, 18)]
+    tests += [(2_000_000_000 - 2, 12), (1_000_000_000, 17), (50_000_002, 17), (1024, 18)]
     jobs = [gf.Job.prefix(b, n, 3 * B + 7 * (i % 3)) for i, (b, n) in enumerate(tests)]
     with MixedBatch(jobs, B=B, tuner=Autotuner(squarings=4, replays=1)) as mb:
         res = mb.run()
         canon_mix = mb.residues()
         plans = mb.plans()
         assert set(plans) == {j.n for j in jobs}
+        assert plans[17] < 200                               # a base outside the packed range
         assert all(r.gl_ok for r in res)
         assert mb.stats.digit_squarings == sum((1 << j.n) * j.nbits for j in jobs)
     checked = 0
