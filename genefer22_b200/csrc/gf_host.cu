@@ -267,12 +267,36 @@ void set_smem(K kernel, size_t smem)
 }
 
 // `prep` only raises the kernel's shared-memory limit (done outside graph capture).
+// Streaming multiprocessors of the current device (cached per device).
+int sm_count()
+{
+	static std::atomic<int> cache[64];
+	int dev = 0;
+	GFC_CK(cudaGetDevice(&dev));
+	if ((dev < 0) || (dev >= 64)) return 148;
+	int v = cache[dev].load();
+	if (v == 0)
+	{
+		GFC_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+		cache[dev].store(v);
+	}
+	return v;
+}
+
 template <int SET, int LOGN>
 void small_t(const Args &a, int grid, cudaStream_t s, bool prep)
 {
-	using S = SmallShape<SET, LOGN>;
-	if (prep) { set_smem(k_small<SET, LOGN>, S::SMEM); return; }
-	k_small<SET, LOGN><<<grid, S::T, S::SMEM, s>>>(a);
+	using S = SmallShape<SET, LOGN, false>;
+	using SS = SmallShape<SET, LOGN, true>;
+	if (prep)
+	{
+		set_smem(k_small<SET, LOGN, false>, S::SMEM);
+		set_smem(k_small<SET, LOGN, true>, SS::SMEM);
+		return;
+	}
+	// fewer tests than SMs: plane-split passes (more warps per test)
+	if (SS::PSPLIT && (grid < sm_count())) k_small<SET, LOGN, true><<<grid, SS::T, SS::SMEM, s>>>(a);
+	else k_small<SET, LOGN, false><<<grid, S::T, S::SMEM, s>>>(a);
 	after_launch();
 }
 
@@ -288,22 +312,6 @@ void small_set(int logn, const Args &a, int grid, cudaStream_t s, bool prep)
 		case 14: small_t<SET, 14>(a, grid, s, prep); break;
 		default: fail(GFC_ERR_ARG, "single-CTA plan needs 10 <= n <= 14");
 	}
-}
-
-// Streaming multiprocessors of the current device (cached per device).
-int sm_count()
-{
-	static std::atomic<int> cache[64];
-	int dev = 0;
-	GFC_CK(cudaGetDevice(&dev));
-	if ((dev < 0) || (dev >= 64)) return 148;
-	int v = cache[dev].load();
-	if (v == 0)
-	{
-		GFC_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
-		cache[dev].store(v);
-	}
-	return v;
 }
 
 // A register column launch whose one-thread-per-column grid (256 columns and

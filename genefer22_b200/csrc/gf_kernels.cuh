@@ -188,6 +188,9 @@ struct Sched
 // PM_MID_SQ / PM_MID_MUL: r forward stages, pointwise square (or product with
 // the multiplicand at zrow[PL * zstride + (lane << l) + i]), r inverse stages.
 //
+// With PSPLIT a work item is one group of one lane of one plane (items of a
+// plane consecutive, so a warp keeps one prime), W times as many items.
+//
 // IO selects where the group's elements come from and go to: IO_SMEM both in
 // the tile; IO_GIN loads from global memory (gmem + pl gstride + (lane << L) + i,
 // natural order) and stores to the tile; IO_GOUT loads from the tile and
@@ -196,19 +199,26 @@ struct Sched
 // consecutive groups, so each of its 2^r accesses is one coalesced line).
 enum : int { IO_SMEM = 0, IO_GIN = 1, IO_GOUT = 2 };
 
-template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO = IO_SMEM>
+template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO = IO_SMEM, bool PSPLIT = false>
 __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										 uint32_t base_step, const Tables &tab, const uint32_t *__restrict__ zrow,
 										 size_t zstride, uint32_t *gmem = nullptr, size_t gstride = 0, int pl_lo = 0,
 										 int pl_hi = PrimeSet<SET>::W)
 {
-	constexpr int W = PrimeSet<SET>::W;
 	constexpr int E = 1 << r;
 	constexpr int GL = L - r;                 // log2 groups per transform
 	constexpr int STEP = 1 << (L - SIGMA - r);
-	const int items = 1 << (lanes_log + GL);
-	for (int it = threadIdx.x; it < items; it += blockDim.x)
+	const int per_log = lanes_log + GL;
+	const int items = PSPLIT ? ((pl_hi - pl_lo) << per_log) : (1 << per_log);
+	for (int it0 = threadIdx.x; it0 < items; it0 += blockDim.x)
 	{
+		int it = it0, p_first = pl_lo, p_end = pl_hi;
+		if constexpr (PSPLIT)
+		{
+			p_first = pl_lo + (it0 >> per_log);
+			p_end = p_first + 1;
+			it = it0 & ((1 << per_log) - 1);
+		}
 		int lane, g;
 		if (lane_fast) { lane = it & ((1 << lanes_log) - 1); g = it >> lanes_log; }
 		else { g = it & ((1 << GL) - 1); lane = it >> GL; }
@@ -216,7 +226,7 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 		const uint32_t tb = ((base0 + static_cast<uint32_t>(lane) * base_step) << SIGMA) + G.blk;
 		const int base = Map::addr(G.i0, lane);
 #pragma unroll 1
-		for (int pl = pl_lo; pl < pl_hi; ++pl)
+		for (int pl = p_first; pl < p_end; ++pl)
 		{
 			const auto z = prime_rt<SET>(pl);
 			uint32_t *pb = buf + (pl - pl_lo) * pstride + base;
@@ -262,29 +272,31 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 }
 
 // Forward passes 0 .. NP-1 (or NP-2 with SKIP_LAST), a barrier after each.
-template <int SET, int L, bool SKIP_LAST, class Map>
+template <int SET, int L, bool SKIP_LAST, class Map, bool PSPLIT = false>
 __device__ __forceinline__ void run_fwd(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										uint32_t base_step, const Tables &tab, int pl_lo = 0, int pl_hi = PrimeSet<SET>::W)
 {
 	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
 	static_for<0, NP>([&](auto P) {
 		constexpr int p = decltype(P)::value;
-		pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
-															  nullptr, 0, nullptr, 0, pl_lo, pl_hi);
+		pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, lane_fast, base0,
+																			   base_step, tab, nullptr, 0, nullptr, 0,
+																			   pl_lo, pl_hi);
 		__syncthreads();
 	});
 }
 
 // Inverse passes NP-1 (or NP-2 with SKIP_LAST) .. 0.
-template <int SET, int L, bool SKIP_LAST, class Map>
+template <int SET, int L, bool SKIP_LAST, class Map, bool PSPLIT = false>
 __device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										uint32_t base_step, const Tables &tab, int pl_lo = 0, int pl_hi = PrimeSet<SET>::W)
 {
 	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
 	static_for<0, NP>([&](auto Q) {
 		constexpr int p = NP - 1 - decltype(Q)::value;
-		pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, lanes_log, lane_fast, base0, base_step, tab,
-															  nullptr, 0, nullptr, 0, pl_lo, pl_hi);
+		pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, lane_fast, base0,
+																			   base_step, tab, nullptr, 0, nullptr, 0,
+																			   pl_lo, pl_hi);
 		__syncthreads();
 	});
 }
@@ -334,49 +346,59 @@ __device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint
 
 // Row transforms in shared memory: forward (OP_FWD), or forward + pointwise
 // square / product + inverse.
-template <int SET, int L, class Map>
+template <int SET, int L, class Map, bool PSPLIT = false>
 __device__ __forceinline__ void row_core(uint32_t *buf, int pstride, int lanes_log, uint32_t base0, const Tables &tab,
 										 const uint32_t *zrow, size_t zstride, int op)
 {
 	constexpr int PL = Sched<L>::NP - 1;
-	if (op == OP_FWD) { run_fwd<SET, L, false, Map>(buf, pstride, lanes_log, false, base0, 1u, tab); return; }
-	run_fwd<SET, L, true, Map>(buf, pstride, lanes_log, false, base0, 1u, tab);
+	if (op == OP_FWD) { run_fwd<SET, L, false, Map, PSPLIT>(buf, pstride, lanes_log, false, base0, 1u, tab); return; }
+	run_fwd<SET, L, true, Map, PSPLIT>(buf, pstride, lanes_log, false, base0, 1u, tab);
 	if (op == OP_MUL)
-		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map>(buf, pstride, lanes_log, false, base0, 1u, tab, zrow, zstride);
+		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, false, base0,
+																					  1u, tab, zrow, zstride);
 	else
-		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map>(buf, pstride, lanes_log, false, base0, 1u, tab, zrow, zstride);
+		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, false, base0,
+																					 1u, tab, zrow, zstride);
 	__syncthreads();
-	run_inv<SET, L, true, Map>(buf, pstride, lanes_log, false, base0, 1u, tab);
+	run_inv<SET, L, true, Map, PSPLIT>(buf, pstride, lanes_log, false, base0, 1u, tab);
 }
 
 // ------------------------------------------------------------------ k_small
 
-// Single-CTA shape for one prime set: T threads, D = N / T digits each;
-// MINB CTAs per SM bound the register budget.
-template <int SET, int LOGN>
+// Single-CTA shape for one prime set: T0 threads own D = N / T0 digits each
+// (CRT and carry).  With SPLIT (up to n = 12, for launches of fewer tests
+// than SMs) the transform passes run plane-split, a thread per (plane,
+// group), on T = W T0 threads: a lone test is one CTA on one SM, and W times
+// the warps hide W times more latency.  MINB CTAs per SM bound the register
+// budget.
+template <int SET, int LOGN, bool SPLIT = false>
 struct SmallShape
 {
 	static constexpr int W = PrimeSet<SET>::W;
 	static constexpr int N = 1 << LOGN;
 	static constexpr int PN = N + N / 32;                 // padded plane
-	static constexpr int T = (LOGN <= 12) ? (N / 16) : 512;
-	static constexpr int MINB = (T <= 128) ? 4 : ((T == 256) ? 2 : 1);
+	static constexpr int T0 = (LOGN <= 12) ? (N / 16) : 512;
+	static constexpr bool PSPLIT = SPLIT && (LOGN <= 12);
+	static constexpr int T = PSPLIT ? W * T0 : T0;
+	static constexpr int MINB = (T <= 128) ? 4 : ((T <= 256) ? 2 : 1);
 	static constexpr size_t SMEM = size_t(W) * PN * 4 + size_t(T) * 8;
 };
 
-template <int SET, int LOGN>
+template <int SET, int LOGN, bool SPLIT>
 __device__ __forceinline__ void small_body(const Args &a, int t, const TestDesc &d, uint32_t *sm)
 {
-	using S = SmallShape<SET, LOGN>;
-	constexpr int N = S::N, PN = S::PN, T = S::T;
-	constexpr int D = N / T;           // digits per thread (multiple of SEG)
+	using S = SmallShape<SET, LOGN, SPLIT>;
+	constexpr int N = S::N, PN = S::PN, T = S::T, T0 = S::T0;
+	constexpr int D = N / T0;          // digits per owner thread (multiple of SEG)
 	static_assert(D % SEG == 0, "digits per thread");
 	int64_t *const sc = reinterpret_cast<int64_t *>(sm + S::W * PN);
 	const Tables &tab = a.tab[SET];
 	const int tid = threadIdx.x;
+	const bool owner = (tid < T0);     // threads T0 .. T-1 join the transform passes only
 	using MP = RowMap<LOGN>;
 
 	int32_t dg[D];
+	if (owner)
 	{
 		const int4 *src = reinterpret_cast<const int4 *>(d.regs + static_cast<size_t>(a.src) * N + tid * D);
 #pragma unroll
@@ -395,15 +417,18 @@ __device__ __forceinline__ void small_body(const Args &a, int t, const TestDesc 
 		const bool dup = (a.op == OP_SQUARE) ? get_dup(a, d, t, it, active) : false;
 		if (!active) break;
 
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			using Z = ZS<SET, PL>;
+		if (owner)
+		{
+			for_planes<SET>([&](auto PLc) {
+				constexpr int PL = decltype(PLc)::value;
+				using Z = ZS<SET, PL>;
 #pragma unroll
-			for (int i = 0; i < D; ++i) sm[PL * PN + MP::addr(tid * D + i, 0)] = Z::from_int(dg[i]);
-		});
+				for (int i = 0; i < D; ++i) sm[PL * PN + MP::addr(tid * D + i, 0)] = Z::from_int(dg[i]);
+			});
+		}
 		__syncthreads();
 
-		row_core<SET, LOGN, MP>(sm, PN, 0, 1u, tab, d.zp, N, a.op);
+		row_core<SET, LOGN, MP, S::PSPLIT>(sm, PN, 0, 1u, tab, d.zp, N, a.op);
 
 		if (a.op == OP_FWD)
 		{
@@ -413,24 +438,31 @@ __device__ __forceinline__ void small_body(const Args &a, int t, const TestDesc 
 			return;
 		}
 
-		// CRT + carry over this thread's D consecutive digits.
-		int64_t c = 0;
-#pragma unroll
-		for (int i = 0; i < D; ++i)
+		// CRT + carry over each owner's D consecutive digits.
+		if (owner)
 		{
-			uint32_t x[3];
+			int64_t c = 0;
 #pragma unroll
-			for (int pl = 0; pl < PrimeSet<SET>::W; ++pl) x[pl] = sm[pl * PN + MP::addr(tid * D + i, 0)];
-			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
+			for (int i = 0; i < D; ++i)
+			{
+				uint32_t x[3];
+#pragma unroll
+				for (int pl = 0; pl < PrimeSet<SET>::W; ++pl) x[pl] = sm[pl * PN + MP::addr(tid * D + i, 0)];
+				dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
+			}
+			sc[tid] = c;
 		}
-		sc[tid] = c;
 		__syncthreads();
-		const int64_t cin = (tid == 0) ? -sc[T - 1] : sc[tid - 1];
-		if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
+		if (owner)
+		{
+			const int64_t cin = (tid == 0) ? -sc[T0 - 1] : sc[tid - 1];
+			if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
+		}
 		__syncthreads();
 		++done;
 	}
 
+	if (owner)
 	{
 		int4 *dst = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(a.dst) * N + tid * D);
 #pragma unroll
@@ -439,13 +471,14 @@ __device__ __forceinline__ void small_body(const Args &a, int t, const TestDesc 
 	if ((tid == 0) && (a.op == OP_SQUARE) && (a.dup_mode == DUP_BITS)) a.pos[t] -= done;
 }
 
-// One CTA per test of prime set SET; shared memory SmallShape<SET, LOGN>::SMEM.
-template <int SET, int LOGN>
-__global__ void __launch_bounds__(SmallShape<SET, LOGN>::T, SmallShape<SET, LOGN>::MINB) k_small(const Args a)
+// One CTA per test of prime set SET; shared memory SmallShape<SET, LOGN, SPLIT>::SMEM.
+template <int SET, int LOGN, bool SPLIT>
+__global__ void __launch_bounds__(SmallShape<SET, LOGN, SPLIT>::T, SmallShape<SET, LOGN, SPLIT>::MINB)
+	k_small(const Args a)
 {
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.x];
-	small_body<SET, LOGN>(a, t, a.desc[t], sm);
+	small_body<SET, LOGN, SPLIT>(a, t, a.desc[t], sm);
 }
 
 // ------------------------------------------------------------------ k_cluster
