@@ -7,12 +7,15 @@
 //          31-bit primes let add/sub/Montgomery use min() corrections)
 // The primes are the NTT-friendly primes genefer's transforms use
 // (src/transformCPUi32.h:19-21 and src/transformGPU.h:37-105: 125*2^25+1,
-// 243*2^24+1; 127*2^24+1, 63*2^25+1, 15*2^27+1).  Every product below is a
-// Montgomery product with R = 2^32 (Montgomery 1985); residues are always
-// fully reduced to [0, p).
+// 243*2^24+1; 127*2^24+1, 63*2^25+1, 15*2^27+1).  Products of two residues
+// are Montgomery products with R = 2^32 (Montgomery 1985); products by a root
+// of the transform tables are Montgomery products for the 32-bit primes and
+// Shoup products (a precomputed quotient per root, Shoup 2007) for the 31-bit
+// primes; residues are always fully reduced to [0, p).
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 namespace gfc {
 
@@ -75,6 +78,21 @@ template <> struct PrimeSet<2>
 
 // ---------------------------------------------------------------- Zp (one prime)
 
+// A root of the transform tables as its prime's product by it wants it: one
+// word in Montgomery form for the 32-bit primes; for the 31-bit primes the
+// root w in normal form with its Shoup quotient q = floor(w 2^32 / p).
+struct RootM { uint32_t w; };
+struct RootS { uint32_t w, q; };
+
+// a w mod p for a < 2^32, w < p < 2^31 (Shoup): with h = floor(a q / 2^32),
+// a w - h p lies in [0, 2p), so its low 32 bits are exact.
+__device__ __forceinline__ uint32_t shoup_mul(uint32_t a, RootS r, uint32_t p)
+{
+	const uint32_t h = __umulhi(a, r.q);
+	const uint32_t t = a * r.w - h * p;
+	return min(t, t - p);
+}
+
 template <uint32_t P, bool P31>
 struct Zp
 {
@@ -111,6 +129,11 @@ struct Zp
 	{
 		return static_cast<uint32_t>(d) + ((d < 0) ? P : 0u);
 	}
+
+	// a times a table root (a w mod p)
+	using root_t = typename std::conditional<P31, RootS, RootM>::type;
+	__device__ __forceinline__ static uint32_t mulr(uint32_t a, RootS r) { return shoup_mul(a, r, P); }
+	__device__ __forceinline__ static uint32_t mulr(uint32_t a, RootM r) { return mul(a, r.w); }
 };
 
 // The same arithmetic with the prime held in registers, so that one code path
@@ -148,6 +171,10 @@ struct ZpR
 	{
 		return static_cast<uint32_t>(d) + ((d < 0) ? p : 0u);
 	}
+
+	using root_t = typename std::conditional<P31, RootS, RootM>::type;
+	__device__ __forceinline__ uint32_t mulr(uint32_t a, RootS r) const { return shoup_mul(a, r, p); }
+	__device__ __forceinline__ uint32_t mulr(uint32_t a, RootM r) const { return mul(a, r.w); }
 };
 
 // Plane `pl` of prime set SET as register-held arithmetic.

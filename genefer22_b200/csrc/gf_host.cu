@@ -86,27 +86,42 @@ inline uint32_t bitrev(uint32_t k, int n)
 	return r;
 }
 
-// Root tables of one prime for length N = 2^n (layout described in gf_ntt.cuh):
-//   fw[k] = psi^bitrev_n(k) R,  iv[k] = psi^-bitrev_n(k) R  (k >= 1, R = 2^32),
-//   fw[0] = R^2 / N (normalisation c),  iv[0] = psi^(-N/2) c  (K).
-void build_roots(uint32_t p, int n, uint32_t *fw, uint32_t *iv)
+// Words per table entry: the 31-bit primes keep each root with its Shoup
+// quotient (gf_arith.cuh, RootS), the 32-bit primes one Montgomery word.
+inline size_t root_words(uint32_t p) { return (p < (1u << 31)) ? 2 : 1; }
+
+// Entry k of a root table: psi^e in Montgomery form (32-bit primes), or in
+// normal form followed by floor(w 2^32 / p) (31-bit primes).
+inline void put_root(uint32_t *t, size_t k, uint32_t w, uint32_t p)
+{
+	if (root_words(p) == 1) { t[k] = to_mont_h(w, p); return; }
+	t[2 * k] = w;
+	t[2 * k + 1] = static_cast<uint32_t>((static_cast<uint64_t>(w) << 32) / p);
+}
+
+// Root tables of one prime for length N = 2^n (N entries of root_words(p)
+// words; layout in gf_ntt.cuh):
+//   entry k of fw = psi^bitrev_n(k), of iv = psi^-bitrev_n(k)  (k >= 1),
+//   word 0 of fw = R^2 / N (normalisation c), of iv = psi^(-N/2) c (K), in
+//   Montgomery form (R = 2^32).  `pw` is scratch for N + 1 powers.
+void build_roots(uint32_t p, int n, uint32_t *fw, uint32_t *iv, uint32_t *pw)
 {
 	const uint32_t N = 1u << n;
 	const uint32_t psi = powmod_h(primitive_root(p), (p - 1) / (2ull * N), p);
-	std::vector<uint32_t> pw(N + 1);
 	pw[0] = 1;
 	for (uint32_t i = 1; i <= N; ++i) pw[i] = mulmod_h(pw[i - 1], psi, p);
 	if (pw[N] != p - 1) fail(GFC_ERR_ARG, "root table: psi is not a primitive 2N-th root");
 	for (uint32_t k = 1; k < N; ++k)
 	{
 		const uint32_t e = bitrev(k, n);
-		fw[k] = to_mont_h(pw[e], p);
-		iv[k] = to_mont_h(p - pw[N - e], p);
+		put_root(fw, k, pw[e], p);
+		put_root(iv, k, p - pw[N - e], p);
 	}
 	const uint32_t R1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
 	const uint32_t c = mulmod_h(mulmod_h(R1, R1, p), powmod_h(N % p, p - 2, p), p);
 	fw[0] = c;
 	iv[0] = mulmod_h(p - pw[N / 2], c, p);
+	if (root_words(p) == 2) { fw[1] = 0; iv[1] = 0; }
 }
 
 struct DeviceTables
@@ -135,21 +150,24 @@ std::shared_ptr<DeviceTables> get_tables(int device, int n)
 	auto t = std::make_shared<DeviceTables>();
 	t->device = device; t->n = n;
 	const size_t N = size_t(1) << n;
-	GFC_CK(cudaMalloc(&t->d, 10 * N * sizeof(uint32_t)));
-	std::vector<uint32_t> fw(N), iv(N);
+	size_t off[5], total = 0;
+	for (int s = 0; s < 5; ++s) { off[s] = total; total += 2 * root_words(kPrime[s]) * N; }
+	GFC_CK(cudaMalloc(&t->d, total * sizeof(uint32_t)));
+	std::vector<uint32_t> fw(2 * N), iv(2 * N), pw(N + 1);
 	for (int s = 0; s < 5; ++s)
 	{
-		build_roots(kPrime[s], n, fw.data(), iv.data());
-		GFC_CK(cudaMemcpy(t->d + (2 * s) * N, fw.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
-		GFC_CK(cudaMemcpy(t->d + (2 * s + 1) * N, iv.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		const size_t words = root_words(kPrime[s]) * N;
+		build_roots(kPrime[s], n, fw.data(), iv.data(), pw.data());
+		GFC_CK(cudaMemcpy(t->d + off[s], fw.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		GFC_CK(cudaMemcpy(t->d + off[s] + words, iv.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
 	}
 	const int slot0[2] = { 0, 2 };
 	for (int set = 0; set < 2; ++set)
 		for (int pl = 0; pl < 3; ++pl)
 		{
 			const int s = (set == 0 && pl == 2) ? 1 : slot0[set] + pl;   // set 0 has 2 planes; plane 2 unused
-			t->tab[set].fw[pl] = t->d + (2 * s) * N;
-			t->tab[set].iv[pl] = t->d + (2 * s + 1) * N;
+			t->tab[set].fw[pl] = t->d + off[s];
+			t->tab[set].iv[pl] = t->d + off[s] + root_words(kPrime[s]) * N;
 		}
 	g_tab_cache[key] = t;
 	return t;
@@ -181,15 +199,16 @@ std::shared_ptr<DeviceTables> get_tables_packed(int device, int np)
 	auto t = std::make_shared<DeviceTables>();
 	t->device = device; t->n = np;
 	const size_t N = size_t(1) << np;
-	GFC_CK(cudaMalloc(&t->d, 8 * N * sizeof(uint32_t)));
-	std::vector<uint32_t> fw(N), iv(N);
+	const size_t words = 2 * N;                       // 31-bit primes: root and Shoup quotient
+	GFC_CK(cudaMalloc(&t->d, 8 * words * sizeof(uint32_t)));
+	std::vector<uint32_t> fw(words), iv(words), pw(N + 1);
 	for (int pl = 0; pl < 4; ++pl)
 	{
-		build_roots(PrimeSet<2>::p[pl], np, fw.data(), iv.data());
-		GFC_CK(cudaMemcpy(t->d + (2 * pl) * N, fw.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
-		GFC_CK(cudaMemcpy(t->d + (2 * pl + 1) * N, iv.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice));
-		t->tab[2].fw[pl] = t->d + (2 * pl) * N;
-		t->tab[2].iv[pl] = t->d + (2 * pl + 1) * N;
+		build_roots(PrimeSet<2>::p[pl], np, fw.data(), iv.data(), pw.data());
+		GFC_CK(cudaMemcpy(t->d + (2 * pl) * words, fw.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		GFC_CK(cudaMemcpy(t->d + (2 * pl + 1) * words, iv.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		t->tab[2].fw[pl] = t->d + (2 * pl) * words;
+		t->tab[2].iv[pl] = t->d + (2 * pl + 1) * words;
 	}
 	g_tab_cache[key] = t;
 	return t;
@@ -1581,12 +1600,13 @@ namespace {
 constexpr int NA_MIN_LOGN = 12, NA_MAX_LOGN = 16, NA_LR = 4;
 constexpr size_t NA_N = size_t(1) << NA_MAX_LOGN;
 // Layout in 32-bit words.
-constexpr size_t NA_OFF_TAB = 0;                                  // 5 primes x (forward, inverse) x N
-constexpr size_t NA_OFF_PLANES = NA_OFF_TAB + 10 * NA_N;          // 3 planes x N
+constexpr size_t NA_OFF_TAB = 0;                                  // 5 primes x (forward, inverse) x N entries
+constexpr size_t NA_TAB_WORDS = 2 * (2 * 1 + 3 * 2) * NA_N;       // 1 word per entry (32-bit primes), 2 (31-bit)
+constexpr size_t NA_OFF_PLANES = NA_OFF_TAB + NA_TAB_WORDS;       // 3 planes x N
 constexpr size_t NA_OFF_CARRY = NA_OFF_PLANES + 3 * NA_N;         // N/16 int64 carries
 constexpr size_t NA_OFF_DESC = NA_OFF_CARRY + NA_N / 8;           // one TestDesc
 constexpr size_t NA_OFF_MISC = NA_OFF_DESC + 128;                 // test index, position, error word
-constexpr size_t NA_WORDS = NA_OFF_MISC + 64;                     // 3.44 MB
+constexpr size_t NA_WORDS = NA_OFF_MISC + 64;                     // 5.01 MB
 static_assert(sizeof(TestDesc) <= 128 * sizeof(uint32_t), "descriptor slot");
 
 static __device__ __align__(256) uint32_t g_na_scratch[NA_WORDS];
@@ -1599,7 +1619,16 @@ struct NaDevice
 };
 std::mutex g_na_mu;
 NaDevice g_na_dev[NA_MAX_DEVICES];
-uint32_t g_na_pw[NA_N + 1], g_na_fw[NA_N], g_na_iv[NA_N];   // host staging for the root tables
+uint32_t g_na_pw[NA_N + 1], g_na_fw[2 * NA_N], g_na_iv[2 * NA_N];   // host staging for the root tables
+
+// Word offset of prime s's forward table in the scratch array (its inverse
+// table follows it).
+size_t na_tab_off(int s)
+{
+	size_t o = NA_OFF_TAB;
+	for (int i = 0; i < s; ++i) o += 2 * root_words(kPrime[i]) * NA_N;
+	return o;
+}
 
 // Smallest generator of (Z/pZ)* without heap use (p - 1 has < 10 prime factors).
 uint32_t na_primitive_root(uint32_t p)
@@ -1628,13 +1657,14 @@ void na_build_roots(uint32_t p, int n)
 	for (uint32_t k = 1; k < N; ++k)
 	{
 		const uint32_t e = bitrev(k, n);
-		g_na_fw[k] = to_mont_h(g_na_pw[e], p);
-		g_na_iv[k] = to_mont_h(p - g_na_pw[N - e], p);
+		put_root(g_na_fw, k, g_na_pw[e], p);
+		put_root(g_na_iv, k, p - g_na_pw[N - e], p);
 	}
 	const uint32_t R1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
 	const uint32_t c = mulmod_h(mulmod_h(R1, R1, p), powmod_h(N % p, p - 2, p), p);
 	g_na_fw[0] = c;
 	g_na_iv[0] = mulmod_h(p - g_na_pw[N / 2], c, p);
+	if (root_words(p) == 2) { g_na_fw[1] = 0; g_na_iv[1] = 0; }
 }
 
 // Per-device set-up (first call on a device): the device address of the
@@ -1657,8 +1687,10 @@ NaDevice &na_setup(int device, int n)
 		for (int s = 0; s < 5; ++s)
 		{
 			na_build_roots(kPrime[s], n);
-			GFC_CK(cudaMemcpy(nd.base + NA_OFF_TAB + (2 * s) * NA_N, g_na_fw, N * sizeof(uint32_t), cudaMemcpyHostToDevice));
-			GFC_CK(cudaMemcpy(nd.base + NA_OFF_TAB + (2 * s + 1) * NA_N, g_na_iv, N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+			const size_t rw = root_words(kPrime[s]);
+			GFC_CK(cudaMemcpy(nd.base + na_tab_off(s), g_na_fw, rw * N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+			GFC_CK(cudaMemcpy(nd.base + na_tab_off(s) + rw * NA_N, g_na_iv, rw * N * sizeof(uint32_t),
+							  cudaMemcpyHostToDevice));
 		}
 		nd.tab_n = n;
 	}
@@ -1710,8 +1742,8 @@ GFC_API int gfc_square_noalloc(const int32_t *in, int32_t *out, uint32_t b, uint
 			for (int pl = 0; pl < 3; ++pl)
 			{
 				const int k = (st == 0 && pl == 2) ? 1 : slot0[st] + pl;
-				a.tab[st].fw[pl] = base + NA_OFF_TAB + (2 * k) * NA_N;
-				a.tab[st].iv[pl] = base + NA_OFF_TAB + (2 * k + 1) * NA_N;
+				a.tab[st].fw[pl] = base + na_tab_off(k);
+				a.tab[st].iv[pl] = base + na_tab_off(k) + root_words(kPrime[k]) * NA_N;
 			}
 		a.n = static_cast<int>(n);
 		a.lr = NA_LR;

@@ -46,10 +46,14 @@ struct TestDesc
 	int32_t set;            // prime set: 0 (W = 2), 1 (W = 3), 2 (W = 4, packed digits)
 };
 
+// Root tables per prime (entries as load_twiddles reads them: one word in
+// Montgomery form for 32-bit primes, root and Shoup quotient for 31-bit
+// primes); word 0 of fw is the normalisation c, word 0 of iv the constant K
+// of the last inverse stage, both in Montgomery form.
 struct Tables
 {
-	const uint32_t *fw[4];  // forward roots, Montgomery form; fw[p][0] = normalisation c
-	const uint32_t *iv[4];  // inverse roots, Montgomery form; iv[p][0] = K (last stage)
+	const uint32_t *fw[4];  // forward roots
+	const uint32_t *iv[4];  // inverse roots
 };
 
 struct Args
@@ -919,7 +923,7 @@ __device__ __forceinline__ void fwd_thread(const Z &z, uint32_t (&x)[1 << L], ui
 #pragma unroll
 		for (int blk = 0; blk < (1 << s0); ++blk)
 		{
-			uint32_t w[(1 << r) - 1];
+			typename Z::root_t w[(1 << r) - 1];
 			load_twiddles<r>(w, (base << s0) + static_cast<uint32_t>(blk), tw);
 #pragma unroll
 			for (int t = 0; t < r; ++t)
@@ -950,7 +954,7 @@ __device__ __forceinline__ void inv_thread(const Z &z, uint32_t (&x)[1 << L], ui
 #pragma unroll
 		for (int blk = 0; blk < (1 << s0); ++blk)
 		{
-			uint32_t w[(1 << r) - 1];
+			typename Z::root_t w[(1 << r) - 1];
 			load_twiddles<r>(w, (base << s0) + static_cast<uint32_t>(blk), twi);
 #pragma unroll
 			for (int t = r - 1; t >= 0; --t)
@@ -1495,8 +1499,12 @@ __device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, 
 	}
 }
 
+// 16-row columns hold 32 digits and 15 two-word roots per thread: three CTAs
+// per SM leave them 85 registers (the inverse kernel's tile fits three anyway).
+__host__ __device__ constexpr int pcol_min_blocks(int lr) { return (lr >= 4) ? 3 : 4; }
+
 template <int LR>
-__global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_fwd(const Args a)
+__global__ void __launch_bounds__(PCOL_THREADS, pcol_min_blocks(LR)) k_pcol_fwd(const Args a)
 {
 	__shared__ int32_t sm[(1 << LR) * (2 * PCOL_THREADS + 2 * PCOL_THREADS / SEG)];
 	const int t = a.tests[blockIdx.y];
@@ -1508,7 +1516,7 @@ __global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_fwd(const Args a)
 }
 
 template <int LR>
-__global__ void __launch_bounds__(PCOL_THREADS, 4) k_pcol_inv(const Args a)
+__global__ void __launch_bounds__(PCOL_THREADS, pcol_min_blocks(LR)) k_pcol_inv(const Args a)
 {
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];

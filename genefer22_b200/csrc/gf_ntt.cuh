@@ -22,30 +22,35 @@
 namespace gfc {
 
 // Z: arithmetic of one prime (Zp with the prime as a constant, or ZpR with
-// the prime in registers).
-template <class Z>
-__device__ __forceinline__ void bfly_ct(const Z &z, uint32_t &a, uint32_t &b, uint32_t w)
+// the prime in registers); R: its root type (Z::root_t).
+template <class Z, class R>
+__device__ __forceinline__ void bfly_ct(const Z &z, uint32_t &a, uint32_t &b, R w)
 {
-	const uint32_t t = z.mul(b, w);
+	const uint32_t t = z.mulr(b, w);
 	b = z.sub(a, t);
 	a = z.add(a, t);
 }
 
-template <class Z>
-__device__ __forceinline__ void bfly_gs(const Z &z, uint32_t &a, uint32_t &b, uint32_t wi)
+template <class Z, class R>
+__device__ __forceinline__ void bfly_gs(const Z &z, uint32_t &a, uint32_t &b, R wi)
 {
 	const uint32_t t = z.sub(a, b);
 	a = z.add(a, b);
-	b = z.mul(t, wi);
+	b = z.mulr(t, wi);
 }
 
-// The twiddles of one radix-2^r group: w[2^t - 1 + sb] = tw[(tbase << t) + sb]
-// for stage t < r of the group and sb < 2^t.  The 2^t words of stage t are
-// consecutive and start at a multiple of 2^t words, so stages t >= 2 load as
-// 16-byte vectors and stage 1 as one 8-byte vector (root tables start on
-// 32-byte boundaries).
+// Root tables: entry idx of a table is one word (RootM: Montgomery form, the
+// 32-bit primes) or two words at 2 idx, 2 idx + 1 (RootS: the root and its
+// Shoup quotient, the 31-bit primes); entry 0 holds the normalisation
+// constant (word 0, Montgomery form, for the Montgomery product).
+//
+// The twiddles of one radix-2^r group: w[2^t - 1 + sb] = entry (tbase << t) + sb
+// for stage t < r of the group and sb < 2^t.  The 2^t entries of stage t are
+// consecutive and start at a multiple of 2^t entries, so they load as 16-byte
+// vectors (one 8-byte vector for the smallest stages; tables start on 32-byte
+// boundaries).
 template <int r>
-__device__ __forceinline__ void load_twiddles(uint32_t (&w)[(1 << r) - 1], uint32_t tbase, const uint32_t *__restrict__ tw)
+__device__ __forceinline__ void load_twiddles(RootM (&w)[(1 << r) - 1], uint32_t tbase, const uint32_t *__restrict__ tw)
 {
 #pragma unroll
 	for (int t = 0; t < r; ++t)
@@ -57,16 +62,41 @@ __device__ __forceinline__ void load_twiddles(uint32_t (&w)[(1 << r) - 1], uint3
 			for (int v = 0; v < (1 << t) / 4; ++v)
 			{
 				const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p) + v);
-				w[(1 << t) - 1 + 4 * v] = u.x; w[(1 << t) + 4 * v] = u.y;
-				w[(1 << t) + 1 + 4 * v] = u.z; w[(1 << t) + 2 + 4 * v] = u.w;
+				w[(1 << t) - 1 + 4 * v].w = u.x; w[(1 << t) + 4 * v].w = u.y;
+				w[(1 << t) + 1 + 4 * v].w = u.z; w[(1 << t) + 2 + 4 * v].w = u.w;
 			}
 		}
 		else if (t == 1)
 		{
 			const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
-			w[1] = u.x; w[2] = u.y;
+			w[1].w = u.x; w[2].w = u.y;
 		}
-		else w[0] = __ldg(p);
+		else w[0].w = __ldg(p);
+	}
+}
+
+template <int r>
+__device__ __forceinline__ void load_twiddles(RootS (&w)[(1 << r) - 1], uint32_t tbase, const uint32_t *__restrict__ tw)
+{
+#pragma unroll
+	for (int t = 0; t < r; ++t)
+	{
+		const uint32_t *p = tw + (static_cast<size_t>(tbase) << (t + 1));
+		if (t >= 1)
+		{
+#pragma unroll
+			for (int v = 0; v < (1 << t) / 2; ++v)
+			{
+				const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p) + v);
+				w[(1 << t) - 1 + 2 * v] = RootS{ u.x, u.y };
+				w[(1 << t) + 2 * v] = RootS{ u.z, u.w };
+			}
+		}
+		else
+		{
+			const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+			w[0] = RootS{ u.x, u.y };
+		}
 	}
 }
 
@@ -76,7 +106,7 @@ __device__ __forceinline__ void load_twiddles(uint32_t (&w)[(1 << r) - 1], uint3
 template <class Z, int r>
 __device__ __forceinline__ void fwd_reg(const Z &z, uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ tw)
 {
-	uint32_t w[(1 << r) - 1];
+	typename Z::root_t w[(1 << r) - 1];
 	load_twiddles<r>(w, tbase, tw);
 #pragma unroll
 	for (int t = 0; t < r; ++t)
@@ -98,7 +128,7 @@ template <class Z, int r>
 __device__ __forceinline__ void inv_reg(const Z &z, uint32_t (&x)[1 << r], uint32_t tbase, const uint32_t *__restrict__ twi,
 										bool norm, uint32_t c_norm, uint32_t k_norm)
 {
-	uint32_t w[(1 << r) - 1];
+	typename Z::root_t w[(1 << r) - 1];
 	load_twiddles<r>(w, tbase, twi);
 #pragma unroll
 	for (int t = r - 1; t >= 0; --t)

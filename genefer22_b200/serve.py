@@ -58,8 +58,11 @@ def slot_bytes(n: int, num_regs: int = NUM_REGS) -> int:
 
 
 def table_bytes(n: int) -> int:
-    """Root tables of size n, shared by every batch of that size on a device."""
-    return 10 * 4 * (1 << int(n))
+    """Root tables of size n, shared by every batch of that size on a device:
+    the two 32-bit primes at one word per root, the three 31-bit primes at two
+    (root and Shoup quotient), forward and inverse (16 N words), and the four
+    primes of packed digits on N/2 points at two words per root (8 N words)."""
+    return 24 * 4 * (1 << int(n))
 
 
 def exponent_bytes(nbits: int) -> int:
