@@ -31,14 +31,19 @@ __global__ void __launch_bounds__(256) k_probe_mulmod(uint32_t *out, int iters, 
 	if (acc == 0x12345678u) out[t] = acc;   // keeps the chains live
 }
 
-// Radix-2 butterfly throughput (one Montgomery product + add + sub).
+// Radix-2 butterfly throughput, with the root product the engine's transforms
+// use for the prime set: a Montgomery product for the 32-bit primes, a Shoup
+// product (root and quotient) for the 31-bit primes; then add + sub.
 template <int SET>
 __global__ void __launch_bounds__(256) k_probe_bfly(uint32_t *out, int iters, uint32_t seed)
 {
 	using Z = gfc::Zp<gfc::PrimeSet<SET>::p[0], gfc::PrimeSet<SET>::P31>;
 	uint32_t a[CHAINS], b[CHAINS];
 	const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-	const uint32_t w = (seed * 747796405u + 2891336453u) % Z::p;
+	typename Z::root_t w;
+	w.w = (seed * 747796405u + 2891336453u) % Z::p;
+	if constexpr (gfc::PrimeSet<SET>::P31)
+		w = gfc::RootS{ w.w, static_cast<uint32_t>((static_cast<uint64_t>(w.w) << 32) / Z::p) };
 #pragma unroll
 	for (int c = 0; c < CHAINS; ++c) { a[c] = (t * 2654435761u + c * 40503u) % Z::p; b[c] = (a[c] ^ 0x9e3779b9u) % Z::p; }
 	for (int i = 0; i < iters; ++i)
@@ -46,7 +51,7 @@ __global__ void __launch_bounds__(256) k_probe_bfly(uint32_t *out, int iters, ui
 #pragma unroll
 		for (int c = 0; c < CHAINS; ++c)
 		{
-			const uint32_t tt = Z::mul(b[c], w);
+			const uint32_t tt = Z::mulr(b[c], w);
 			b[c] = Z::sub(a[c], tt);
 			a[c] = Z::add(a[c], tt);
 		}
@@ -79,7 +84,8 @@ double time_kernel(K kernel, uint32_t *buf, int blocks, int iters)
 
 // Measures Montgomery products/s and radix-2 butterflies/s on `device` for
 // the 32-bit (set 0) and 31-bit (set 1) primes: out[0..3] = mulmod32,
-// mulmod31, butterfly32, butterfly31 per second.  Returns 0 or -2.
+// mulmod31, butterfly32 (Montgomery root product), butterfly31 (Shoup root
+// product) per second.  Returns 0 or -2.
 extern "C" __attribute__((visibility("default"))) int gfc_probe_int_throughput(int device, double *out)
 {
 	if (cudaSetDevice(device) != cudaSuccess) return -2;

@@ -217,8 +217,10 @@ int gfc_batch_time_kernels(gfc_batch *bt, uint32_t reps, float *ms);
 
 /* Integer-pipe probe (no counterpart in the reference): Montgomery products
  * and radix-2 butterflies per second on `device`, out[0..3] = product with
- * the 32-bit primes, product with the 31-bit primes, butterfly 32-bit,
- * butterfly 31-bit.  The roofline denominator for the squaring kernels. */
+ * the 32-bit primes, product with the 31-bit primes, butterfly 32-bit
+ * (Montgomery root product), butterfly 31-bit (Shoup root product, as the
+ * transforms of the 31-bit prime sets run it).  The roofline denominator for
+ * the squaring kernels. */
 int gfc_probe_int_throughput(int device, double *out);
 
 /* ------------------------------------------------------------------ squaring without allocation
