@@ -96,6 +96,18 @@ __device__ __forceinline__ bool exp_bit(const uint32_t *ebits, int64_t i)
 	return ((__ldg(&ebits[i >> 5]) >> (i & 31)) & 1u) != 0;
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be scheduled while the previous kernel of its stream is
+// still running; it waits here (griddepcontrol.wait returns once every
+// prerequisite grid has completed and its memory is visible, at once without
+// one) before it touches memory, then lets the next kernel of the stream be
+// scheduled as its own CTAs retire.  Every kernel starts with this.
+__device__ __forceinline__ void pdl_wait()
+{
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // dup flag of squaring j (DUP_BITS: bit pos - j of the exponent); false with
 // `active` cleared when the test has no squaring left.
 __device__ __forceinline__ bool get_dup(const Args &a, const TestDesc &d, int t, int j, bool &active)
@@ -480,6 +492,7 @@ template <int SET, int LOGN, bool SPLIT>
 __global__ void __launch_bounds__(SmallShape<SET, LOGN, SPLIT>::T, SmallShape<SET, LOGN, SPLIT>::MINB)
 	k_small(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.x];
 	small_body<SET, LOGN, SPLIT>(a, t, a.desc[t], sm);
@@ -652,6 +665,7 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 template <int LQ>
 __global__ void __launch_bounds__(ClusterShape<LQ>::T, 2) k_cluster(const Args a, int ntests)
 {
+	pdl_wait();
 	namespace cg = cooperative_groups;
 	using S = ClusterShape<LQ>;
 	extern __shared__ __align__(16) uint32_t sm[];
@@ -868,6 +882,7 @@ __device__ __forceinline__ void col_inv_body(const Args &a, const TestDesc &d, b
 template <int LR>
 __global__ void __launch_bounds__(col_threads(LR)) k_col_fwd(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -881,6 +896,7 @@ __global__ void __launch_bounds__(col_threads(LR)) k_col_fwd(const Args a)
 template <int LC>
 __global__ void __launch_bounds__(row_threads(LC)) k_row(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -896,6 +912,7 @@ __global__ void __launch_bounds__(row_threads(LC)) k_row(const Args a)
 template <int LR>
 __global__ void __launch_bounds__(col_threads(LR)) k_col_inv(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1044,6 +1061,7 @@ __device__ __forceinline__ void mid_body(const Args &a, const TestDesc &d, uint3
 template <int LR2, bool INV>
 __global__ void __launch_bounds__(col_threads(LR2)) k_mid(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1086,6 +1104,7 @@ __device__ __forceinline__ void midr_body(const Args &a, const TestDesc &d, int 
 template <int LR2, bool INV>
 __global__ void __launch_bounds__(MIDR_THREADS) k_midr(const Args a)
 {
+	pdl_wait();
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
 	bool active;
@@ -1203,6 +1222,7 @@ __device__ __forceinline__ void col_inv_reg_body(const Args &a, const TestDesc &
 template <int LR>
 __global__ void __launch_bounds__(COLR_THREADS) k_colr_fwd(const Args a)
 {
+	pdl_wait();
 	__shared__ int32_t sm[(1 << LR) * (COLR_THREADS + COLR_THREADS / SEG)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1221,6 +1241,7 @@ struct ColRegShape
 template <int LR>
 __global__ void __launch_bounds__(COLR_THREADS) k_colr_inv(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1323,6 +1344,7 @@ __device__ __forceinline__ void col_inv_split_body(const Args &a, const TestDesc
 template <int LR>
 __global__ void __launch_bounds__(WMAX * CS_T) k_colr_fwd_s(const Args a)
 {
+	pdl_wait();
 	__shared__ int32_t sm[(1 << LR) * (CS_T + CS_T / SEG)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1335,6 +1357,7 @@ __global__ void __launch_bounds__(WMAX * CS_T) k_colr_fwd_s(const Args a)
 template <int LR>
 __global__ void __launch_bounds__(WMAX * CS_T) k_colr_inv_s(const Args a)
 {
+	pdl_wait();
 	__shared__ __align__(16) uint32_t sm[WMAX * (1 << LR) * (CS_T + CS_T / 16)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1506,6 +1529,7 @@ __host__ __device__ constexpr int pcol_min_blocks(int lr) { return (lr >= 4) ? 3
 template <int LR>
 __global__ void __launch_bounds__(PCOL_THREADS, pcol_min_blocks(LR)) k_pcol_fwd(const Args a)
 {
+	pdl_wait();
 	__shared__ int32_t sm[(1 << LR) * (2 * PCOL_THREADS + 2 * PCOL_THREADS / SEG)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1518,6 +1542,7 @@ __global__ void __launch_bounds__(PCOL_THREADS, pcol_min_blocks(LR)) k_pcol_fwd(
 template <int LR>
 __global__ void __launch_bounds__(PCOL_THREADS, pcol_min_blocks(LR)) k_pcol_inv(const Args a)
 {
+	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1659,6 +1684,7 @@ __device__ __forceinline__ void pcol_inv_split_body(const Args &a, const TestDes
 template <int LR>
 __global__ void __launch_bounds__(4 * PCS_T) k_pcol_fwd_s(const Args a)
 {
+	pdl_wait();
 	__shared__ int32_t sm[(1 << LR) * (2 * PCS_T + 2 * PCS_T / SEG)];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1671,6 +1697,7 @@ __global__ void __launch_bounds__(4 * PCS_T) k_pcol_fwd_s(const Args a)
 template <int LR>
 __global__ void __launch_bounds__(4 * PCS_T) k_pcol_inv_s(const Args a)
 {
+	pdl_wait();
 	__shared__ __align__(16) uint32_t sm[4 * PColShapeS<LR>::PS];
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
@@ -1683,6 +1710,7 @@ __global__ void __launch_bounds__(4 * PCS_T) k_pcol_inv_s(const Args a)
 // Pending packed carries of register a.dst absorbed (a.n = n: digits).
 __global__ void __launch_bounds__(256) k_pfixup(const Args a)
 {
+	pdl_wait();
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
 	bool active;
@@ -1715,6 +1743,7 @@ __global__ void __launch_bounds__(256) k_pfixup(const Args a)
 // the last carry: b^N = -1).
 __global__ void __launch_bounds__(256) k_fixup(const Args a)
 {
+	pdl_wait();
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
 	bool active;
@@ -1744,6 +1773,7 @@ __global__ void __launch_bounds__(256) k_fixup(const Args a)
 // transform::squareMul (src/transformCPUi32.h:774-797).  |digit m| < 2^62.
 __global__ void __launch_bounds__(256) k_mulscalar(const Args a, int32_t m)
 {
+	pdl_wait();
 	const int t = a.tests[blockIdx.y];
 	const TestDesc &d = a.desc[t];
 	const size_t N = size_t(1) << a.n;
@@ -1770,6 +1800,7 @@ __global__ void __launch_bounds__(256) k_mulscalar(const Args a, int32_t m)
 // reg[dst] = a (digit 0), 0 elsewhere, for every test of the launch.
 __global__ void k_set(const Args a, int32_t value)
 {
+	pdl_wait();
 	const int t = a.tests[blockIdx.y];
 	const size_t N = size_t(1) << a.n;
 	int32_t *r = a.desc[t].regs + static_cast<size_t>(a.dst) * N;
@@ -1780,6 +1811,7 @@ __global__ void k_set(const Args a, int32_t value)
 // reg[dst] = reg[src] for every test of the launch.
 __global__ void k_copy(const Args a)
 {
+	pdl_wait();
 	const int t = a.tests[blockIdx.y];
 	const size_t N = size_t(1) << a.n;
 	const int4 *s = reinterpret_cast<const int4 *>(a.desc[t].regs + static_cast<size_t>(a.src) * N);
@@ -1792,6 +1824,7 @@ __global__ void k_copy(const Args a)
 // k_small advances its own tests the same way).
 __global__ void k_pos_sub(int64_t *pos, const int32_t *tests, int ntests, int count)
 {
+	pdl_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < ntests)
 	{
