@@ -232,7 +232,7 @@ int gfc_probe_int_throughput(int device, double *out);
  * at device address `out` (may equal `in`), on `stream` (NULL: the default
  * stream) of `device`.  The input digits must satisfy |d| <= b/2 + 1.
  *  - All scratch (root tables, transform planes, carries) lives in one
- *    static device array of 3.44 MB that every GPU loading the library holds
+ *    static device array of 5.01 MB that every GPU loading the library holds
  *    until the process exits; the call makes no cudaMalloc/cudaFree and no
  *    allocating library call.  Hence 12 <= n <= 16; larger n returns
  *    GFC_ERR_ARG.
