@@ -81,15 +81,7 @@ __device__ __forceinline__ void for_planes(F &&f)
 	if constexpr (PrimeSet<SET>::W >= 4) f(std::integral_constant<int, 3>{});
 }
 
-template <int B, int E, class F>
-__device__ __forceinline__ void static_for(F &&f)
-{
-	if constexpr (B < E)
-	{
-		f(std::integral_constant<int, B>{});
-		static_for<B + 1, E>(f);
-	}
-}
+
 
 __device__ __forceinline__ bool exp_bit(const uint32_t *ebits, int64_t i)
 {
@@ -1101,8 +1093,11 @@ __device__ __forceinline__ void midr_body(const Args &a, const TestDesc &d, int 
 	for (int k = 0; k < (1 << LR2); ++k) p[k * C] = x[k];
 }
 
+// 32-word columns (lr2 = 5) fit four CTAs per SM in 128 registers.
+__host__ __device__ constexpr int midr_min_blocks(int lr2) { return (lr2 == 5) ? 4 : 1; }
+
 template <int LR2, bool INV>
-__global__ void __launch_bounds__(MIDR_THREADS) k_midr(const Args a)
+__global__ void __launch_bounds__(MIDR_THREADS, midr_min_blocks(LR2)) k_midr(const Args a)
 {
 	pdl_wait();
 	const int t = a.tests[blockIdx.y];

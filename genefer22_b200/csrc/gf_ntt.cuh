@@ -21,6 +21,18 @@
 
 namespace gfc {
 
+// f(integral_constant<B>), ..., f(integral_constant<E - 1>): a loop whose index
+// is a compile-time constant in every iteration.
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f)
+{
+	if constexpr (B < E)
+	{
+		f(std::integral_constant<int, B>{});
+		static_for<B + 1, E>(f);
+	}
+}
+
 // Z: arithmetic of one prime (Zp with the prime as a constant, or ZpR with
 // the prime in registers); R: its root type (Z::root_t).
 template <class Z, class R>
@@ -130,32 +142,29 @@ __device__ __forceinline__ void inv_reg(const Z &z, uint32_t (&x)[1 << r], uint3
 {
 	typename Z::root_t w[(1 << r) - 1];
 	load_twiddles<r>(w, tbase, twi);
-#pragma unroll
-	for (int t = r - 1; t >= 0; --t)
-	{
-		const int half = 1 << (r - 1 - t);
-#pragma unroll
-		for (int sb = 0; sb < (1 << t); ++sb)
+	static_for<0, r>([&](auto Q) {
+		constexpr int t = r - 1 - decltype(Q)::value;
+		constexpr int half = 1 << (r - 1 - t);
+		if ((t == 0) && norm)
 		{
-			if ((t == 0) && norm)
-			{
 #pragma unroll
-				for (int m = 0; m < half; ++m)
-				{
-					uint32_t &a = x[m], &b = x[m + half];
-					const uint32_t d = z.sub(a, b);
-					a = z.mul(z.add(a, b), c_norm);
-					b = z.mul(d, k_norm);
-				}
-			}
-			else
+			for (int m = 0; m < half; ++m)
 			{
+				uint32_t &a = x[m], &b = x[m + half];
+				const uint32_t d = z.sub(a, b);
+				a = z.mul(z.add(a, b), c_norm);
+				b = z.mul(d, k_norm);
+			}
+		}
+		else
+		{
+#pragma unroll
+			for (int sb = 0; sb < (1 << t); ++sb)
 #pragma unroll
 				for (int m = 0; m < half; ++m)
 					bfly_gs(z, x[sb * 2 * half + m], x[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
-			}
 		}
-	}
+	});
 }
 
 // Shared-memory address maps.  addr(i, lane) places element i of transform
