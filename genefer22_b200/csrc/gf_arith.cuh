@@ -323,21 +323,21 @@ __device__ __forceinline__ int32_t carry_small(int64_t s, const CarryK &K, int64
 // A coefficient of the packed transform is D = d0 + b d1 for two consecutive
 // balanced base-b digits.  After the inverse transform its CRT value is f V
 // (f = 1, or 2 for a doubled square), |V| < M/2 with M = p1 p2 p3 p4 < 2^124.
-// Garner gives V = a1 + p1 a2 + p1 p2 a3 + p1 p2 p3 a4 (a_k < p_k, minus M
-// when V > M/2).  Every weight w = f p1 ... p_{k-1} and f M is written in base
-// b on the host (limbs < b < 2^28), so that
-//     f V = sum_j U_j b^j,   U_j = sum_k a_k w_{k,j} - [V > M/2] (f M)_j,
-// a sum of products of 31- and 28-bit numbers.  The limbs shrink with j
-// (w1 < 2^33, w2 < 2^64, w3 < 2^95 and b >= 2^20 give |U_0|, |U_1| < 2^60.6,
-// |U_2| < 2^60, |U_3| < 2^59.1, |U_4| < 2^45, |U_5|, |U_6| < 2^28), and a
-// window position p collects U_{p-2i} of at most four coefficients i plus the
-// carry of the digit before it, so every position stays below 2^61.4 in
-// magnitude: the U_j are added to the window unsplit, two digits are completed
-// per coefficient (one 64-bit division each), and what remains after a
-// 16-digit segment (positions 16 .. 20) is the segment's carry, five values
-// below 2^62 added to the next segment's first five digits.
+// Garner gives V = a1 + p1 a2 + p1 p2 a3 + p1 p2 p3 a4' with a_k < p_k and
+// a4' = a4, or a4 - p4 when the value a1 + ... + p1 p2 p3 a4 exceeds M/2 (then
+// it is V + M, and M = p1 p2 p3 p4).  Every weight w = f p1 ... p_{k-1} is
+// written in base b on the host (limbs < b < 2^28), so that
+//     f V = sum_{j<5} U_j b^j,   U_j = sum_k a_k w_{k,j},
+// a sum of products of (signed) 31- and 28-bit numbers.  The limbs shrink
+// with j (w1 < 2^33, w2 < 2^64, w3 < 2^95 and b >= 2^20 give |U_0|, |U_1| <
+// 2^60.6, |U_2| < 2^60, |U_3| < 2^59.1, |U_4| < 2^45), and a window position p
+// collects U_{p-2i} of at most three coefficients i plus the carry of the
+// digit before it, so every position stays below 2^61.4 in magnitude: the U_j
+// are added to the window unsplit, two digits are completed per coefficient
+// (one 64-bit division each), and what remains after a 16-digit segment
+// (positions 16 .. 20) is the segment's carry, five values below 2^62 added to
+// the next segment's first five digits.
 
-constexpr int PK_LIMBS = 7;     // base-b limbs of f M (b >= 2^20, f M < 2^125)
 constexpr int PK_CARRY = 5;     // carry values per 16-digit segment
 
 // Per-test constants of the packed CRT + carry (host-computed); index f - 1.
@@ -346,7 +346,6 @@ struct PackK
 	uint32_t w1[2][2];          // limbs 0..1 of f p1
 	uint32_t w2[2][4];          // limbs 0..3 of f p1 p2
 	uint32_t w3[2][5];          // limbs 0..4 of f p1 p2 p3
-	uint32_t m[2][PK_LIMBS];    // limbs of f M
 	uint32_t bm[4];             // b mod p_k in Montgomery form (packing d0 + b d1)
 };
 
@@ -376,26 +375,22 @@ __device__ __forceinline__ void crt_garner4(uint32_t (&x)[4])
 }
 
 // Adds f V (mixed-radix digits g from crt_garner4) to the window at
-// positions 0..6.
+// positions 0..4.
 __device__ __forceinline__ void crt_window_g(const uint32_t (&g)[4], int dup, const PackK &P, int64_t (&win)[7])
 {
 	const int f = dup;                                                       // index f - 1
-	const int64_t zm = static_cast<int64_t>(g[3] >> 31);
-	const uint64_t A1 = g[0], A2 = g[1], A3 = g[2], A4 = g[3] & 0x7fffffffu;
-	int64_t U[PK_LIMBS];
-	U[0] = static_cast<int64_t>((A1 << dup) + A2 * P.w1[f][0] + A3 * P.w2[f][0] + A4 * P.w3[f][0]) - zm * P.m[f][0];
-	U[1] = static_cast<int64_t>(A2 * P.w1[f][1] + A3 * P.w2[f][1] + A4 * P.w3[f][1]) - zm * P.m[f][1];
-	U[2] = static_cast<int64_t>(A3 * P.w2[f][2] + A4 * P.w3[f][2]) - zm * P.m[f][2];
-	U[3] = static_cast<int64_t>(A3 * P.w2[f][3] + A4 * P.w3[f][3]) - zm * P.m[f][3];
-	U[4] = static_cast<int64_t>(A4 * P.w3[f][4]) - zm * P.m[f][4];
-	U[5] = -zm * P.m[f][5];
-	U[6] = -zm * P.m[f][6];
-#pragma unroll
-	for (int j = 0; j < PK_LIMBS; ++j) win[j] += U[j];
+	const uint64_t A1 = g[0], A2 = g[1], A3 = g[2];
+	// the top digit, less p4 for the centred value V > M/2 (M = p1 p2 p3 p4)
+	const int64_t A4 = static_cast<int64_t>(g[3] & 0x7fffffffu) - ((g[3] >> 31) ? static_cast<int64_t>(Crt<2>::p4) : 0);
+	win[0] += static_cast<int64_t>((A1 << dup) + A2 * P.w1[f][0] + A3 * P.w2[f][0]) + A4 * static_cast<int64_t>(P.w3[f][0]);
+	win[1] += static_cast<int64_t>(A2 * P.w1[f][1] + A3 * P.w2[f][1]) + A4 * static_cast<int64_t>(P.w3[f][1]);
+	win[2] += static_cast<int64_t>(A3 * P.w2[f][2]) + A4 * static_cast<int64_t>(P.w3[f][2]);
+	win[3] += static_cast<int64_t>(A3 * P.w2[f][3]) + A4 * static_cast<int64_t>(P.w3[f][3]);
+	win[4] += A4 * static_cast<int64_t>(P.w3[f][4]);
 }
 
 // Adds the CRT value of one packed coefficient (residues x[4]) times f to the
-// window at positions 0..6.
+// window at positions 0..4.
 __device__ __forceinline__ void crt_window(const uint32_t x[4], int dup, const PackK &P, int64_t (&win)[7])
 {
 	uint32_t g[4] = { x[0], x[1], x[2], x[3] };

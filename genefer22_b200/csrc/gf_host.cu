@@ -263,13 +263,12 @@ void base_limbs(u128 w, uint32_t b, uint32_t *out, int count)
 PackK pack_constants(uint32_t b)
 {
 	PackK P{};
-	const u128 p1 = PrimeSet<2>::p[0], p2 = PrimeSet<2>::p[1], p3 = PrimeSet<2>::p[2], p4 = PrimeSet<2>::p[3];
+	const u128 p1 = PrimeSet<2>::p[0], p2 = PrimeSet<2>::p[1], p3 = PrimeSet<2>::p[2];
 	for (int f = 1; f <= 2; ++f)
 	{
 		base_limbs(f * p1, b, P.w1[f - 1], 2);
 		base_limbs(f * p1 * p2, b, P.w2[f - 1], 4);
 		base_limbs(f * p1 * p2 * p3, b, P.w3[f - 1], 5);
-		base_limbs(f * p1 * p2 * p3 * p4, b, P.m[f - 1], PK_LIMBS);
 	}
 	for (int k = 0; k < 4; ++k)
 	{
