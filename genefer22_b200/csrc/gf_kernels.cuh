@@ -7,16 +7,23 @@
 // (src/transform.h:59; CPU reference src/transformCPUi32.h:857-868).
 //
 // Resting state of a register: N signed int32 digits in natural order with
-// |d| <= b/2 + 1 (balanced).  Two kernel shapes:
+// |d| <= b/2 + 1 (balanced).  Kernel shapes:
 //   * k_small (n <= 14): one CTA owns one test; the W planes live in shared
 //     memory and the CTA can run many squarings without touching HBM.
-//   * four-step (n >= 15): N = R x C.  k_col_fwd does the first log2 R stages
-//     on column tiles, k_row the remaining stages + pointwise + inverse on
-//     rows, k_col_inv the last inverse stages, CRT and the carry inside
-//     16-digit segments, and k_fixup adds each segment's carry to the next.
+//   * k_cluster: one test in the shared memory of a thread-block cluster.
+//   * four-step: N = R x C.  The column-forward kernel (k_colr_fwd, k_col_fwd)
+//     does the first log2 R stages, k_row the remaining stages + pointwise +
+//     inverse on rows, the column-inverse kernel the last inverse stages, CRT
+//     and the carry inside 16-digit segments (each segment's carry is added
+//     to the next by the next column-forward pass, or by k_fixup).
+//   * six-step: the column transform is split into a 16-point register pass
+//     and a middle pass (k_midr, k_mid).
+//   * packed digits (prime set 2): two digits per coefficient of a transform
+//     of N/2 points over four primes (k_pcol_fwd, k_row, k_pcol_inv).
+// Column kernels come in a one-thread-per-column form and a plane-split form
+// (_s: a thread per plane and column) for launches that would leave SMs idle.
 // Every kernel serves all tests of a batch in one launch; each CTA picks the
-// code path of its test's prime set (W = 2 or 3) and processes the W planes
-// of a radix group together.
+// code path of its test's prime set (W = 2, 3 or 4).
 #pragma once
 
 #include <type_traits>
