@@ -47,17 +47,17 @@ inline void after_launch()
 	if (e != cudaSuccess) fail(GFC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
 }
 
-// kernel<<<grid, block, smem, s>>>(args), outside stream capture with
-// programmatic stream serialization: the grid may be scheduled while the
-// previous kernel of the stream drains, and waits at its start (pdl_wait)
-// until that kernel has completed, so memory effects keep the order of plain
-// launches while the launch and ramp-up overlap the previous kernel's tail
-// (one squaring per call at n = 16, 17: +38 %, +41 % measured on one B200).
-// Graphs are captured with plain launches: with programmatic edges the
-// replays of some plans ran up to 9 % slower (n = 13, 14, 23) and of others
-// 2-4 % faster.
-template <class... KArgs, class... Args>
-void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const Args &... args)
+// kernel<<<grid, block, smem, s>>>(a) with programmatic stream serialization:
+// the grid may be scheduled while the previous kernel of the stream drains,
+// and waits at its start (pdl_wait) until that kernel has completed, so memory
+// effects keep the order of plain launches while the launch and ramp-up
+// overlap the previous kernel's tail (one squaring per call at n = 16, 17:
+// +38 %, +41 % measured on one B200).  Under stream capture only when
+// a.pdl_graph is set: graph replays with programmatic edges measured 2-4 %
+// faster for packed plans with middle passes of at most 2^5 points
+// (n = 17..22) and up to 9 % slower for others (unpacked n = 13, 14; plan 306).
+template <class K>
+void launch_pdl(K *kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, const Args &a)
 {
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = grid;
@@ -70,8 +70,8 @@ void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cu
 	cfg.attrs = at;
 	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
 	GFC_CK(cudaStreamIsCapturing(s, &cs));
-	cfg.numAttrs = (cs == cudaStreamCaptureStatusNone) ? 1 : 0;
-	GFC_CK(cudaLaunchKernelEx(&cfg, kernel, args...));
+	cfg.numAttrs = ((cs == cudaStreamCaptureStatusNone) || (a.pdl_graph != 0)) ? 1 : 0;
+	GFC_CK(cudaLaunchKernelEx(&cfg, kernel, a));
 	after_launch();
 }
 
@@ -766,6 +766,7 @@ Args make_args(const gfc_batch &bt)
 	a.n = bt.n;
 	a.lr = bt.lr;
 	a.num_regs = static_cast<int>(bt.num_regs);
+	a.pdl_graph = (bt.packed && (bt.six <= 5)) ? 1 : 0;
 	return a;
 }
 

@@ -74,6 +74,7 @@ struct Args
 	int num_regs, src, dst; // registers
 	int op, dup_mode, count, j;  // operation, dup source, squarings (k_small), squaring index in block
 	int fix;                // four-step column-forward: register src has pending segment carries
+	int pdl_graph;          // host only: graph-captured launches keep programmatic edges
 };
 
 template <int SET, int PL>
