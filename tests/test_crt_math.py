@@ -1,0 +1,126 @@
+"""The integer identities the squaring kernels rely on, restated with Python
+integers (CPU only; the kernels themselves are checked against the oracle by
+the GPU tests):
+
+* the Shoup product by a table root (gf_arith.cuh, shoup_mul): for a 31-bit
+  prime p, a < 2^32 and w < p with q = floor(w 2^32 / p), a w - h p with
+  h = floor(a q / 2^32) lies in [0, 2p), below 2^32, and is a w mod p;
+* the packed CRT (crt_garner4, crt_window_g): the top-down test on Garner's
+  mixed-radix digits decides V > M/2, and with the top digit a4 - p4 when it
+  does, f V = sum_{j<5} U_j b^j for the base-b limbs of f p1, f p1 p2,
+  f p1 p2 p3, with |U_j| and every window position inside the stated bounds.
+"""
+import math
+
+import numpy as np
+import pytest
+
+P31 = (127 * 2**24 + 1, 63 * 2**25 + 1, 15 * 2**27 + 1)                 # prime set 1
+P2 = (127 * 2**24 + 1, 63 * 2**25 + 1, 249 * 2**23 + 1, 15 * 2**27 + 1)  # prime set 2 (packed)
+M2 = P2[0] * P2[1] * P2[2] * P2[3]
+
+
+def shoup(a, w, p):
+    q = (w << 32) // p
+    h = (a * q) >> 32
+    return a * w - h * p
+
+
+@pytest.mark.parametrize("p", sorted(set(P31 + P2)))
+def test_shoup_product_range(p):
+    rng = np.random.default_rng(p % 1000)
+    cases = [(2**32 - 1, p - 1), (2**32 - 1, 1), (0, p - 1), (p - 1, p - 1), (p, p - 1)]
+    cases += [(int(a), int(w)) for a, w in zip(rng.integers(0, 2**32, 4000, dtype=np.uint64),
+                                              rng.integers(0, p, 4000, dtype=np.uint64))]
+    for a, w in cases:
+        t = shoup(a, w, p)
+        assert 0 <= t < 2 * p < 2**32
+        assert t % p == (a * w) % p
+
+
+def garner4(v):
+    """Mixed-radix digits of 0 <= v < M2 (what crt_garner4 computes from the
+    residues v mod p_k)."""
+    p1, p2, p3, p4 = P2
+    x = [v % p for p in P2]
+    a1 = x[0]
+    a2 = (x[1] - a1) * pow(p1, -1, p2) % p2
+    a3 = (x[2] - a1 - p1 * a2) * pow(p1 * p2, -1, p3) % p3
+    a4 = (x[3] - a1 - p1 * a2 - p1 * p2 * a3) * pow(p1 * p2 * p3, -1, p4) % p4
+    return a1, a2, a3, a4
+
+
+def top_down_z(a1, a2, a3, a4):
+    """crt_garner4's test of V > M/2 from the top digit down."""
+    p1, p2, p3, p4 = P2
+    low = a2 * p1 + a1
+    rest_hi = a3 > (p3 - 1) // 2 or (a3 == (p3 - 1) // 2 and low > (p1 * p2) // 2)
+    return a4 > (p4 - 1) // 2 or (a4 == (p4 - 1) // 2 and rest_hi)
+
+
+def limbs(w, b, count):
+    out = []
+    for _ in range(count):
+        out.append(w % b)
+        w //= b
+    assert w == 0
+    return out
+
+
+def window_terms(digits, z, f, b):
+    """U_0..U_4 of crt_window_g for mixed-radix digits, flag z and f = 1, 2."""
+    p1, p2, p3, p4 = P2
+    a1, a2, a3, a4 = digits
+    A4 = a4 - (p4 if z else 0)
+    w1, w2, w3 = limbs(f * p1, b, 2), limbs(f * p1 * p2, b, 4), limbs(f * p1 * p2 * p3, b, 5)
+    return [f * a1 + a2 * w1[0] + a3 * w2[0] + A4 * w3[0],
+            a2 * w1[1] + a3 * w2[1] + A4 * w3[1],
+            a3 * w2[2] + A4 * w3[2],
+            a3 * w2[3] + A4 * w3[3],
+            A4 * w3[4]]
+
+
+def boundary_values():
+    half = M2 // 2
+    return [0, 1, half - 1, half, half + 1, M2 - 1, M2 - 2, (M2 - 1) // 2, P2[0] * P2[1] * P2[2] * ((P2[3] - 1) // 2)]
+
+
+def test_top_down_test_is_v_above_half_m():
+    rng = np.random.default_rng(5)
+    vals = boundary_values() + [int.from_bytes(rng.bytes(16), "little") % M2 for _ in range(3000)]
+    for v in vals:
+        assert top_down_z(*garner4(v)) == (v > M2 // 2), v
+
+
+@pytest.mark.parametrize("b", [2**20, 2**20 + 2, 3_000_002, 2**24, 100_000_000, 2**28 - 2])
+def test_centred_window_expansion(b):
+    rng = np.random.default_rng(b % 997)
+    vals = boundary_values() + [int.from_bytes(rng.bytes(16), "little") % M2 for _ in range(1500)]
+    for v in vals:
+        d = garner4(v)
+        z = top_down_z(*d)
+        vc = v - M2 if z else v                       # the centred value, |vc| <= M/2
+        for f in (1, 2):
+            U = window_terms(d, z, f, b)
+            assert sum(u * b**j for j, u in enumerate(U)) == f * vc
+
+
+@pytest.mark.parametrize("b", [2**20, 2**22, 2**24 + 2, 2**26, 2**28 - 2])
+def test_window_bounds(b):
+    """Worst case over the digit ranges: each U_j at its stated bound, every
+    window position (U_j of at most three coefficients, j = p - 2i) below
+    2^61.4, so that carry_wide (|s| < 2^62) covers it with the carry added."""
+    p1, p2, p3, p4 = P2
+    worst = [0.0] * 5
+    for f in (1, 2):
+        for a4, z in ((p4 - 1, False), (0, True), ((p4 - 1) // 2, True)):
+            U = window_terms((p1 - 1, p2 - 1, p3 - 1, a4), z, f, b)
+            for j, u in enumerate(U):
+                worst[j] = max(worst[j], math.log2(abs(u)) if u else 0.0)
+    bounds = (60.6, 60.6, 60.0, 59.1, 45.0)
+    for j in range(5):
+        assert worst[j] < bounds[j], (j, worst[j])
+    even = math.log2(2**worst[0] + 2**worst[2] + 2**worst[4])
+    odd = math.log2(2**worst[1] + 2**worst[3])
+    carry = max(even, odd) - math.log2(b)             # the digit before's carry into a position
+    assert math.log2(2**max(even, odd) + 2**carry) < 61.4 < 62
