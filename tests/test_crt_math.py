@@ -8,7 +8,10 @@ the GPU tests):
 * the packed CRT (crt_garner4, crt_window_g): the top-down test on Garner's
   mixed-radix digits decides V > M/2, and with the top digit a4 - p4 when it
   does, f V = sum_{j<5} U_j b^j for the base-b limbs of f p1, f p1 p2,
-  f p1 p2 p3, with |U_j| and every window position inside the stated bounds.
+  f p1 p2 p3, with |U_j| and every window position inside the stated bounds;
+* the fused CRT + carry of prime sets 0 and 1 (crt_carry<SET>): one 64-bit
+  division by b and per-test constants give the balanced digit and the carry
+  of f V + c exactly.
 """
 import math
 
@@ -124,3 +127,77 @@ def test_window_bounds(b):
     odd = math.log2(2**worst[1] + 2**worst[3])
     carry = max(even, odd) - math.log2(b)             # the digit before's carry into a position
     assert math.log2(2**max(even, odd) + 2**carry) < 61.4 < 62
+
+
+# ---- the fused CRT + carry of prime sets 0 and 1 (gf_arith.cuh crt_carry<SET>)
+
+P0 = (125 * 2**25 + 1, 243 * 2**24 + 1)
+MASK = 2**64 - 1
+
+
+def carry_constants(b, primes):
+    """carry_constants() of the host code: T is the top Garner weight."""
+    T = primes[0] if len(primes) == 2 else primes[0] * primes[1]
+    M = math.prod(primes)
+    k = (2**56 + b - 1) // b
+    return dict(b=b, h=b // 2, binv=MASK // b, k=k, kb=k * b,
+                q=[(f * T) // b for f in (1, 2)], r=[(f * T) % b for f in (1, 2)],
+                mq=[((f * M) // b) & MASK for f in (1, 2)], mr=[(f * M) % b for f in (1, 2)])
+
+
+def divb64(n, K):
+    assert 0 <= n <= MASK
+    q = (n * K["binv"]) >> 64
+    r = n - q * K["b"]
+    if r >= K["b"]:
+        q, r = q + 1, r - K["b"]
+    assert 0 <= r < K["b"]
+    return q, r
+
+
+def crt_carry(x, dup, K, c, primes):
+    """The kernel's arithmetic (uint64 wrap-around as on the device)."""
+    if len(primes) == 2:
+        p1, p2 = primes
+        a_top = (x[1] - x[0]) * pow(p1, -1, p2) % p2
+        low = x[0]
+        z = a_top * p1 + x[0] > (p1 * p2) // 2
+    else:
+        p1, p2, p3 = primes
+        a2 = (x[1] - x[0]) * pow(p1, -1, p2) % p2
+        a_top = (x[2] - x[0] - p1 * a2) * pow(p1 * p2, -1, p3) % p3
+        low = a2 * p1 + x[0]
+        z = a_top > (p3 - 1) // 2 or (a_top == (p3 - 1) // 2 and low > (p1 * p2) // 2)
+    U = (low << dup) + K["r"][dup] * a_top + K["h"] + ((K["b"] - K["mr"][dup]) if z else 0)
+    assert U <= MASK
+    qv, rv = divb64((U + (c & MASK) + K["kb"]) & MASK, K)
+    cout = (qv + K["q"][dup] * a_top - ((K["mq"][dup] + 1) if z else 0) - K["k"]) & MASK
+    cout = cout - 2**64 if cout >= 2**63 else cout
+    return rv - K["h"], cout
+
+
+@pytest.mark.parametrize("primes", [P0, P31], ids=["set0", "set1"])
+@pytest.mark.parametrize("b", [8, 1_000, 65_538, 22_000_000, 1_000_000_000, 2**31 - 2])
+def test_fused_crt_carry_is_exact(primes, b):
+    """digit + b * carry_out = f V_c + carry_in with the digit in [-b/2, b - b/2)
+    and V_c the centred CRT value, for carries up to 2^54 in magnitude and
+    every product coefficient the engine can form: |V_c| <= N (b/2 + 1)^2 with
+    N <= 2^23, inside M/2 (the width rule picks the prime set that way; the
+    carry out then stays far below 2^63, which makes the quotient assembled
+    modulo 2^64 exact)."""
+    M = math.prod(primes)
+    K = carry_constants(b, primes)
+    bound = min(M // 2, 2**23 * (b // 2 + 1) ** 2)
+    rng = np.random.default_rng(b % 1009 + len(primes))
+    vcs = [0, 1, -1, bound, -bound, bound - 1, -(bound - 1)] + \
+          [int.from_bytes(rng.bytes(16), "little") % (2 * bound + 1) - bound for _ in range(800)]
+    cs = [0, 1, -1, 2**54, -2**54] + [int(c) for c in rng.integers(-2**54, 2**54, 800)]
+    for i, vc in enumerate(vcs):
+        v = vc % M
+        x = [v % p for p in primes]
+        assert (v - M if v > M // 2 else v) == vc
+        for dup in (0, 1):
+            c = cs[(i * 7 + dup) % len(cs)]
+            d, cout = crt_carry(x, dup, K, c, primes)
+            assert -(b // 2) <= d < b - b // 2
+            assert d + b * cout == (dup + 1) * vc + c, (v, dup, c)
