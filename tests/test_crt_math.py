@@ -11,7 +11,11 @@ the GPU tests):
   f p1 p2 p3, with |U_j| and every window position inside the stated bounds;
 * the fused CRT + carry of prime sets 0 and 1 (crt_carry<SET>): one 64-bit
   division by b and per-test constants give the balanced digit and the carry
-  of f V + c exactly.
+  of f V + c exactly;
+* the absorption of a segment's carry into the next 16 digits (absorb,
+  absorb5): it fits for every carry the engine produces, keeps the value and
+  leaves every digit within b/2 + 1 (the resting bound the exact ranges
+  assume).
 """
 import math
 
@@ -201,3 +205,86 @@ def test_fused_crt_carry_is_exact(primes, b):
             d, cout = crt_carry(x, dup, K, c, primes)
             assert -(b // 2) <= d < b - b // 2
             assert d + b * cout == (dup + 1) * vc + c, (v, dup, c)
+
+
+# ---- carry absorption into a 16-digit segment (gf_kernels.cuh absorb, gf_arith.cuh absorb5)
+
+SEG = 16
+
+
+def carry_balanced(s, b):
+    """carry_small / carry_wide: the balanced digit of s and floor((s + b/2) / b)."""
+    h = b // 2
+    q = (s + h) // b
+    return s + h - q * b - h, q
+
+
+def absorb(dg, c, b):
+    """absorb<D>: reduce while |c| > 1, then leave the last +-1 in the next
+    digit unreduced; False if the carry did not fit."""
+    dg = list(dg)
+    for k in range(len(dg)):
+        if c == 0:
+            break
+        if abs(c) > 1:
+            dg[k], c = carry_balanced(dg[k] + c, b)
+        else:
+            dg[k] += c
+            c = 0
+    return c == 0, dg
+
+
+def absorb5(dg, cin, b):
+    """absorb5<D>: a packed segment carry (cin[k] at digit k, k < 5)."""
+    dg = list(dg)
+    q, done = 0, False
+    for k in range(len(dg)):
+        if done:
+            continue
+        if k >= 5 and -1 <= q <= 1:
+            dg[k] += q
+            q, done = 0, True
+            continue
+        dg[k], q = carry_balanced(dg[k] + (cin[k] if k < 5 else 0) + q, b)
+    return done or q == 0, dg
+
+
+def value(dg, b):
+    return sum(d * b**k for k, d in enumerate(dg))
+
+
+@pytest.mark.parametrize("b", [8, 10, 1024, 65_538, 22_000_000, 1_000_000_000, 2**31 - 2])
+def test_absorb_segment_carry(b):
+    """The carry out of a segment (at most the largest product coefficient,
+    2^23 (b/2 + 1)^2 times 2 for a doubled square, over b, plus one) fits in
+    the next segment, the value is kept, and every digit ends within b/2 + 1."""
+    h = b // 2
+    cmax = (2 * 2**23 * (h + 1) ** 2) // b + 1
+    rng = np.random.default_rng(b % 1013)
+    for _ in range(400):
+        dg = [int(x) for x in rng.integers(-h, b - h, SEG)]
+        c = int(rng.integers(-cmax, cmax + 1)) if _ > 3 else (cmax, -cmax, 1, -1)[_]
+        ok, out = absorb(dg, c, b)
+        assert ok, (b, c)
+        assert value(out, b) == value(dg, b) + c
+        assert max(abs(d) for d in out) <= h + 1
+
+
+@pytest.mark.parametrize("b", [2**20, 2**20 + 2, 5_000_002, 2**24, 100_000_000, 2**28 - 2])
+def test_absorb5_packed_segment_carry(b):
+    """A packed segment carry (five window positions below 2^62 in magnitude)
+    fits in the next 16-digit segment, the value is kept, and every digit ends
+    within b/2 + 1."""
+    h = b // 2
+    lim = int(2**61.4)
+    rng = np.random.default_rng(b % 1019)
+    for i in range(400):
+        dg = [int(x) for x in rng.integers(-h, b - h, SEG)]
+        if i < 4:
+            cin = [(lim, -lim)[i % 2]] * 5 if i < 2 else [(lim, -lim)[i % 2]] * 3 + [0, 0]
+        else:
+            cin = [int.from_bytes(rng.bytes(8), "little") % (2 * lim + 1) - lim for _ in range(5)]
+        ok, out = absorb5(dg, cin, b)
+        assert ok, (b, cin)
+        assert value(out, b) == value(dg, b) + value(cin, b)
+        assert max(abs(d) for d in out) <= h + 1
