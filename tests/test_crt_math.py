@@ -288,3 +288,16 @@ def test_absorb5_packed_segment_carry(b):
         assert ok, (b, cin)
         assert value(out, b) == value(dg, b) + value(cin, b)
         assert max(abs(d) for d in out) <= h + 1
+
+
+@pytest.mark.parametrize("b", [2, 3, 8, 1023, 2**20 + 7, 2**28 - 2, 2**31 - 1])
+def test_barrett_division_by_b(b):
+    """divb64: q = mulhi(n, floor((2^64 - 1) / b)) is floor(n / b) or one less
+    for every n < 2^64, so one compare completes it."""
+    binv = MASK // b
+    rng = np.random.default_rng(b % 97)
+    ns = [0, 1, b - 1, b, MASK, MASK - 1, MASK - b, (MASK // b) * b, (MASK // b) * b - 1] + \
+         [int.from_bytes(rng.bytes(8), "little") for _ in range(3000)]
+    for n in ns:
+        q = (n * binv) >> 64
+        assert n // b - q in (0, 1), (n, b)
