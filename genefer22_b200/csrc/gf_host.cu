@@ -1724,6 +1724,13 @@ GFC_API int gfc_square_noalloc(const int32_t *in, int32_t *out, uint32_t b, uint
 		if ((in == nullptr) || (out == nullptr)) fail(GFC_ERR_ARG, "square_noalloc: null digit pointer");
 		if ((n < NA_MIN_LOGN) || (n > NA_MAX_LOGN))
 			fail(GFC_ERR_ARG, "square_noalloc: n must satisfy 12 <= n <= 16 (size of the static scratch array)");
+		{
+			// the device-to-device copy below needs in == out or disjoint ranges
+			const uintptr_t pi = reinterpret_cast<uintptr_t>(in), po = reinterpret_cast<uintptr_t>(out);
+			const uintptr_t bytes = (uintptr_t(1) << n) * sizeof(int32_t);
+			if ((pi != po) && (((pi < po) ? po - pi : pi - po) < bytes))
+				fail(GFC_ERR_ARG, "square_noalloc: in and out must be equal or disjoint");
+		}
 		if ((b < 8) || (b >= (1u << 31))) fail(GFC_ERR_ARG, "square_noalloc: base b must satisfy 8 <= b < 2^31");
 		const int set = choose_set(b, static_cast<int>(n));
 		if (set < 0) fail(GFC_ERR_RANGE, "square_noalloc: (b, n) is outside the exact range of the RNS prime sets");

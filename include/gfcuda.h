@@ -229,8 +229,9 @@ int gfc_probe_int_throughput(int device, double *out);
  * or allocator lock, processes with a device-memory budget fixed at start-up,
  * hosts that forbid allocation after initialisation): count squarings (dup
  * as in gfc_square_dup) of the N = 2^n digits at device address `in`, result
- * at device address `out` (may equal `in`), on `stream` (NULL: the default
- * stream) of `device`.  The input digits must satisfy |d| <= b/2 + 1.
+ * at device address `out` (equal to `in`, or a disjoint range: a partial
+ * overlap returns GFC_ERR_ARG), on `stream` (NULL: the default stream) of
+ * `device`.  The input digits must satisfy |d| <= b/2 + 1.
  *  - All scratch (root tables, transform planes, carries) lives in one
  *    static device array of 5.01 MB that every GPU loading the library holds
  *    until the process exits; the call makes no cudaMalloc/cudaFree and no
@@ -238,7 +239,10 @@ int gfc_probe_int_throughput(int device, double *out);
  *    GFC_ERR_ARG.
  *  - The first call on a device resolves the array's device address and
  *    builds its root tables (again whenever n changes); make that first call
- *    before any stream capture.
+ *    before any stream capture.  The library remembers per device that the
+ *    tables are built; a cudaDeviceReset discards the array's contents
+ *    without the library seeing it, so after resetting a device a process
+ *    must not call this entry point on that device again.
  *  - Every call shares the array: calls that overlap on the GPU (other
  *    streams, other host threads without ordering) race.  The call waits for
  *    `stream` before returning and reports a device-side carry failure as

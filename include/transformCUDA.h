@@ -7,15 +7,19 @@
  * Failures of the engine raise std::runtime_error, as genefer's OpenCL
  * backend does (src/ocl.h:166-175).
  *
- * The transform kind written into context files is EKind::NTT3 unless the
- * including code defines TRANSFORM_CUDA_KIND to another EKind enumerator
- * (for example after adding `CUDA` to transform::EKind, src/transform.h:45).
- * The payload carries its own tag (GFC_CONTEXT_KIND), so a context written by
- * another backend with the same kind is rejected by readContext.
+ * Context files: genefer reads the transform's kind only from the first word
+ * of a context (src/transformGPU.h:1127-1150).  This backend writes
+ * GFC_CONTEXT_KIND there, a value that no transform::EKind enumerator
+ * (src/transform.h:45, 0..11) takes, so a context written by the OpenCL build
+ * (EKind::NTT2 / NTT3) or a CPU build fails readContext at the kind check,
+ * and a context of this backend fails theirs.  The `transform` base still
+ * needs an EKind: NTT3 unless the including code defines TRANSFORM_CUDA_KIND
+ * (for example after adding `CUDA` to transform::EKind).
  */
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -72,13 +76,16 @@ public:
 	void mul() override { check(gfc_mul(_h), "mul"); }
 	void copy(const size_t dst, const size_t src) const override { check(gfc_copy(_h, dst, src), "copy"); }
 
+	// Kind word of this backend's context files (see the file comment).
+	static constexpr int context_kind = static_cast<int>(GFC_CONTEXT_KIND);
+
 	// readContext / saveContext (src/transformGPU.h:1127-1150): kind, then the
 	// registers; num_regs == 0 means every register.
 	bool readContext(file &cFile, const size_t nregs) override
 	{
 		int kind = 0;
 		if (!cFile.read(reinterpret_cast<char *>(&kind), sizeof(kind))) return false;
-		if (kind != static_cast<int>(getKind())) return false;
+		if (kind != context_kind) return false;
 		const size_t num_regs = (nregs != 0) ? nregs : _num_regs;
 		std::vector<char> buf(gfc_context_size(_h, num_regs));
 		if (!cFile.read(buf.data(), buf.size())) return false;
@@ -87,7 +94,7 @@ public:
 
 	void saveContext(file &cFile, const size_t nregs) const override
 	{
-		const int kind = static_cast<int>(getKind());
+		const int kind = context_kind;
 		if (!cFile.write(reinterpret_cast<const char *>(&kind), sizeof(kind))) return;
 		const size_t num_regs = (nregs != 0) ? nregs : _num_regs;
 		std::vector<char> buf(gfc_context_size(_h, num_regs));
@@ -95,6 +102,20 @@ public:
 		cFile.write(buf.data(), buf.size());
 	}
 
-	// Number of RNS primes (2 or 3) the engine chose for (b, n).
+	// transform::getError (src/transform.h:72): the engine's arithmetic is
+	// exact integer arithmetic, so there is no rounding error to report; a carry
+	// that does not fit is an exception from the next synchronising call.
+	double getError() const override { return 0; }
+
+	// transform::info (src/transform.h:73; the OpenCL backend prints its split,
+	// src/transformGPU.h:903-930): the RNS width and kernel plan of this test.
+	void info() const override
+	{
+		unsigned n = 0;
+		while ((size_t(1) << n) < getSize()) ++n;
+		std::printf("transformCUDA: n = %u, b = %u, %d primes, plan %d\n", n, getB(), gfc_width(_h), gfc_batch_plan(_h));
+	}
+
+	// Number of RNS primes (2, 3, or 4 with packed digits) the engine chose for (b, n).
 	int width() const { return gfc_width(_h); }
 };

@@ -4,7 +4,8 @@
  * infrastructure only (used by oracle/Makefile for oracle/_ref).
  *
  * Declares the documented public GMP 6 ABI for the handful of mpz entry
- * points the reference headers and oracle/ref_harness.cpp call.  Each
+ * points the reference headers, oracle/ref_harness.cpp and
+ * oracle/genefer_harness.cpp call.  Each
  * mpz_* name maps to the __gmpz_* symbol exported by libgmp.so.10.
  */
 #pragma once
@@ -51,6 +52,12 @@ typedef const __mpz_struct *mpz_srcptr;
 #define mpz_tstbit __gmpz_tstbit
 #define mpz_add __gmpz_add
 #define mpz_export __gmpz_export
+#define mpz_add_ui __gmpz_add_ui
+#define mpz_addmul __gmpz_addmul
+#define mpz_cmp __gmpz_cmp
+#define mpz_mul __gmpz_mul
+#define mpz_mul_ui __gmpz_mul_ui
+#define mpz_sub __gmpz_sub
 
 void __gmpz_init(mpz_ptr);
 void __gmpz_init_set(mpz_ptr, mpz_srcptr);
@@ -70,6 +77,12 @@ size_t __gmpz_sizeinbase(mpz_srcptr, int);
 int __gmpz_tstbit(mpz_srcptr, mp_bitcnt_t);
 void __gmpz_add(mpz_ptr, mpz_srcptr, mpz_srcptr);
 void *__gmpz_export(void *, size_t *, int, size_t, int, size_t, mpz_srcptr);
+void __gmpz_add_ui(mpz_ptr, mpz_srcptr, unsigned long int);
+void __gmpz_addmul(mpz_ptr, mpz_srcptr, mpz_srcptr);
+int __gmpz_cmp(mpz_srcptr, mpz_srcptr);
+void __gmpz_mul(mpz_ptr, mpz_srcptr, mpz_srcptr);
+void __gmpz_mul_ui(mpz_ptr, mpz_srcptr, unsigned long int);
+void __gmpz_sub(mpz_ptr, mpz_srcptr, mpz_srcptr);
 
 #define mpz_sgn(z) ((z)->_mp_size < 0 ? -1 : (z)->_mp_size > 0)
 

@@ -72,16 +72,19 @@ def main():
     # configuration 4: the first 48 tests of the uneven workload (seed 1004); 40 squarings each
     out["cases"]["c4_uneven_prefix40"] = [run_prefix(b, n, 40) for b, n in uneven_tests(256, seed=1004)[:48]]
     print("c4", flush=True)
-    # configuration 5: n = 15..23 at the per-n limits' scale (seed 1005); 16 squarings each
+    # configuration 5: n = 15..23 at the per-n limits' scale (seed 1005); 48 squarings each.  The
+    # state after k squarings from 1 is 2^e with e < 2^k, so k >= 28 is needed before it
+    # exceeds b^N at n = 23 and wraps; the last 20 or more squarings then work on dense
+    # states with carries across the whole register.
     rng = np.random.default_rng(1005)
     lim = {15: 2_000_000_000, 16: 1_500_000_000, 17: 10**9, 18: 10**9, 19: 70_000_000, 20: 55_000_000,
            21: 45_000_000, 22: 35_000_000, 23: 25_000_000}
     cases = []
     for n in range(15, 24):
         b = int(rng.integers(1024, lim[n])) & ~1
-        cases.append(run_prefix(b, n, 16))
+        cases.append(run_prefix(b, n, 48))
         print("c5", n, flush=True)
-    out["cases"]["c5_serving_prefix16"] = cases
+    out["cases"]["c5_serving_prefix48"] = cases
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1)
 

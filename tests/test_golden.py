@@ -29,7 +29,7 @@ def _oracle_prefix(oracle, c):
 
 def _cheap():
     out = [c for c in GOLDEN["c4_uneven_prefix40"] if c["n"] <= 13][:6]
-    out += GOLDEN["c2_n16_prefix48"][:2] + [c for c in GOLDEN["c5_serving_prefix16"] if c["n"] == 15]
+    out += GOLDEN["c2_n16_prefix48"][:2] + [c for c in GOLDEN["c5_serving_prefix48"] if c["n"] == 15]
     return out
 
 
@@ -38,7 +38,16 @@ def test_oracle_matches_reference_golden(oracle, c):
     assert _oracle_prefix(oracle, c) == (c["res64"], c["old64"], c["hash64"])
 
 
+def test_c5_states_wrap():
+    """Each configuration-5 case squares long enough that the state 2^e (e the exponent
+    prefix, e >= 2^(bits-1)) exceeds b^N and wraps modulo b^N + 1: the later squarings
+    work on dense digits, with carries across the whole register."""
+    import math
+    for c in GOLDEN["c5_serving_prefix48"]:
+        assert 2 ** (c["bits"] - 1) > (1 << c["n"]) * math.log2(c["b"]) * 2 ** 16, c["n"]
+
+
 def test_golden_shapes():
     assert len(GOLDEN["c2_n16_prefix48"]) == 64 and {c["n"] for c in GOLDEN["c2_n16_prefix48"]} == {16}
-    assert {c["n"] for c in GOLDEN["c5_serving_prefix16"]} == set(range(15, 24))
+    assert {c["n"] for c in GOLDEN["c5_serving_prefix48"]} == set(range(15, 24))
     assert all(c["gl"] and not c["isPrp"] for c in GOLDEN["c1_full_n12"])

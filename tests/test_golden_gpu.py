@@ -70,7 +70,7 @@ def test_c4_uneven_batch():
 
 
 def test_c5_serving():
-    cases = GOLDEN["c5_serving_prefix16"]
+    cases = GOLDEN["c5_serving_prefix48"]
     reqs = [Request(i, gf.Job.prefix(c["b"], c["n"], c["bits"]), 0.01 * i) for i, c in enumerate(cases)]
     srv = Server(B=8, budget_bytes=20 * 10**9, validate_group=1, keep_digits=True)
     comps = srv.run(reqs, timeout_s=900)

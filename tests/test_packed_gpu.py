@@ -67,13 +67,21 @@ def test_packed_six_step_vs_oracle(oracle, n, plan, b):
     d = rand_digits(rng, b, 1 << n)
     t.setInt(d)
     o.setInt(d)
-    for dup in (False, True):
+    for k, dup in enumerate((False, True, False)):
         t.squareDup(dup)
         o.squareDup(dup)
-        assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), dup
+        g = t.getInt()
+        assert np.abs(g).max() <= b // 2 + 1
+        assert np.array_equal(canon(g, b), canon(o.getInt(), b)), f"square {k}"
     t.copy(1, 0); o.copy(1, 0)
+    t.squareDup(False); o.squareDup(False)
     t.mul(1); o.mul(1)
     assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), "mul"
+    t.copy(2, 0); o.copy(2, 0)
+    t.initMultiplicand(2); o.initMultiplicand(2)
+    t.squareDup(True); o.squareDup(True)
+    t.mul(); o.mul()
+    assert np.array_equal(canon(t.getInt(), b), canon(o.getInt(), b)), "mul 2"
 
 
 def test_range_refused():

@@ -70,6 +70,18 @@ def test_six_step_plan(oracle, n, plan, b):
     check_ops(oracle, b, n, plan=plan, seed=200 + n + plan, steps=3)
 
 
+# The default unpacked plans of the two largest sizes (106 at n = 22, 107 at n = 23), which
+# serve every base outside the packed-digit range (b < 2^20, or above the packed limit):
+# squarings, dup squarings, mul by a register and initMultiplicand + mul against the oracle.
+# Both bases lie outside the packed range (below 2^20, above 2^28), so they take these plans by
+# default.
+@pytest.mark.parametrize("n,plan", [(22, 106), (23, 107)])
+@pytest.mark.parametrize("b", [SMALL_B // 4, LARGE_B])
+def test_six_step_default_plans_largest_sizes(oracle, n, plan, b):
+    assert Transform(b, n).batch.plan() == plan
+    check_ops(oracle, b, n, plan=plan, seed=300 + n, steps=3)
+
+
 def test_width_choice():
     # unpacked: 2 primes while N (b/2+1)^2 < P1 P2 / 2, else 3; packed digits
     # (the default from n = 16 for bases in the packed range): 4

@@ -56,3 +56,36 @@ def test_square_noalloc_in_place_and_limits():
     torch.cuda.synchronize()
     assert lib().gfc_square_noalloc(_ptr(big), _ptr(big), b, 17, 0, 1, 0, None) == -1
     assert b"12 <= n <= 16" in lib().gfc_last_error()
+
+
+def test_square_noalloc_allocates_nothing():
+    """The point of the entry point: once a device is set up, calls take no device memory,
+    also when a change of n rebuilds the root tables inside the static array.  The warm-up
+    calls load every kernel the later calls launch, so lazy module loading cannot show up
+    as an allocation."""
+    import torch
+    cases = [(1_000_002, 12), (50_000_002, 16)]
+    bufs = [torch.zeros(1 << n, dtype=torch.int32, device="cuda:0") for _, n in cases]
+    torch.cuda.synchronize()
+    for (b, n), buf in zip(cases, bufs):
+        assert lib().gfc_square_noalloc(_ptr(buf), _ptr(buf), b, n, 0, 1, 0, None) == GFC_OK
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(2):
+        for (b, n), buf in zip(cases, bufs):
+            rc = lib().gfc_square_noalloc(_ptr(buf), _ptr(buf), b, n, 1, 2, 0, None)
+            assert rc == GFC_OK, lib().gfc_last_error().decode()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] >= free0
+
+
+def test_square_noalloc_rejects_partial_overlap():
+    import torch
+    b, n = 1_000_002, 12
+    buf = torch.zeros(2 << n, dtype=torch.int32, device="cuda:0")
+    torch.cuda.synchronize()
+    base = buf.data_ptr()
+    half = ctypes.cast(ctypes.c_void_p(base + 4 * (1 << (n - 1))), c_i32p)
+    assert lib().gfc_square_noalloc(_ptr(buf), half, b, n, 0, 1, 0, None) == -1
+    assert b"equal or disjoint" in lib().gfc_last_error()
+    far = ctypes.cast(ctypes.c_void_p(base + 4 * (1 << n)), c_i32p)
+    assert lib().gfc_square_noalloc(_ptr(buf), far, b, n, 0, 1, 0, None) == GFC_OK
