@@ -323,6 +323,8 @@ def run_ours(args):
     tr.sync()
     plain = (1 << N_LOG) * kp / (time.perf_counter() - t0)
 
+    extras = north_star(args, bs) if (world == 1 and not args.no_extras) else None
+
     cpu = None
     if world == 1 and not args.no_cpu:
         try:
@@ -354,6 +356,8 @@ def run_ours(args):
         "plain": {"value": plain, "unit": METRIC, "what": "one test, one gfc_square_dup call per squaring"},
         "batched_over_plain": value / world / plain,
     }
+    if extras is not None:
+        line["north_star"] = extras
     print(json.dumps(line), flush=True)
     if dist is not None:
         del g
@@ -398,58 +402,40 @@ def _plain_rate(b: int, n: int, squarings: int) -> float:
 
 def run_uneven(args):
     """256 tests, n from {12:40%,...,18:2%}, b log-uniform [1024, 2e9) clipped
-    to the per-n limits (seed 1004); one step = one Gerbicz-Li block of
-    1000 squarings of every test, the size classes' graphs in flight together."""
+    to the per-n limits (seed 1004), each running `steps` Gerbicz-Li blocks of
+    1000 squarings, all submitted at once to the native loop: one pool per size
+    class with a slot per test, the classes' graphs in flight together."""
     import torch
     from genefer22_b200.autotune import Autotuner
     from genefer22_b200.genefer import Job
     from genefer22_b200.mixed import MixedBatch, uneven_tests
     torch.cuda.set_device(0)
     tests = uneven_tests(256, seed=1004)
-    nblk = args.warmup + 2 * args.steps + 2
-    jobs = [Job.prefix(b, n, nblk * BLOCK) for b, n in tests]
-    tuner = Autotuner(squarings=8, replays=3)
-    mb = MixedBatch(jobs, B=BLOCK, tuner=tuner)
-    for c in mb.classes:
-        c.prp.load()
-        c.prp.block_graph()
-    streams = [torch.cuda.ExternalStream(c.batch.stream) for c in mb.classes]
-    launch = lambda: [c.prp.block_graph().launch() for c in mb.classes]
-    for _ in range(args.warmup):
-        launch()
-    for c in mb.classes:
-        c.batch.sync()
-    mix_ms = [_device_time(streams, launch, torch) for _ in range(args.steps)]
-    # the same blocks with the classes one after another
-    seq_ms = []
-    for _ in range(args.steps):
-        t = 0.0
-        for c, s in zip(mb.classes, streams):
-            t += _device_time([s], lambda c=c: c.prp.block_graph().launch(), torch)
-        seq_ms.append(t)
-    digits = sum(1 << n for _, n in tests)
-    value = digits * BLOCK * args.steps / (sum(mix_ms) * 1e-3)
+    warm = MixedBatch([Job.prefix(b, n, BLOCK) for b, n in tests], B=BLOCK, tuner=Autotuner())
+    warm.run(validate=False)
+    jobs = [Job.prefix(b, n, args.steps * BLOCK) for b, n in tests]
+    mb = MixedBatch(jobs, B=BLOCK, tuner=Autotuner())
+    with Clocks(0) as ck:
+        res = mb.run(validate=True)
+    st = mb.stats
     per_class = {}
     plain_s = 0.0
-    for c in mb.classes:
-        pr = _plain_rate(c.batch.bases[0], c.n, 200 if c.n <= 16 else 60)
-        plain_s += len(c.index) * (1 << c.n) * BLOCK / pr
-        per_class[c.n] = {"tests": len(c.index), "plan_lr": c.batch.plan(),
-                          "rns_widths": {"2": int(np.sum(c.batch.widths() == 2)), "3": int(np.sum(c.batch.widths() == 3))},
-                          "tuned_us_per_squaring": {str(k): round(v, 2) for k, v in c.tune.us.items()},
-                          "plain_digit_sq_per_s": pr}
-    plain = digits * BLOCK / plain_s
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": float(np.mean(mix_ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic",
+    for n, c in sorted(st.per_class.items()):
+        b0 = next(b for b, m in tests if m == n)
+        pr = _plain_rate(b0, n, 200 if n <= 16 else 60)
+        plain_s += c["digit_squarings"] / pr
+        per_class[n] = {"tests": c["tests"], "plan": c["plan"], "plain_digit_sq_per_s": pr}
+    plain = st.digit_squarings / plain_s
+    line = {"metric": METRIC, "value": st.rate, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": 1,
+            "ms_per_step": st.seconds / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": "uneven batch of 256 tests, n 12..18 (40/20/15/10/8/5/2 %), b log-uniform "
-                                   "[1024,2e9) clipped per n, seed 1004, Gerbicz-Li block of 1000 squarings",
-                       "classes": per_class},
-            "sequential_classes": {"value": digits * BLOCK * args.steps / (sum(seq_ms) * 1e-3),
-                                   "ms_per_step": float(np.mean(seq_ms))},
+                                   "[1024,2e9) clipped per n, seed 1004, Gerbicz-Li block of 1000 squarings, "
+                                   "native loop (one pool per size class)",
+                       "classes": per_class, "timing": "host clock, submission to the last residue read back"},
+            "gl_failures": sum(1 for r in res if not r.gl_ok),
             "plain": {"value": plain, "what": "each test alone, one gfc_square_dup call per squaring"},
-            "mixed_over_plain": value / plain}
-    mb.close()
+            "mixed_over_plain": st.rate / plain, "clocks": ck.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -460,18 +446,16 @@ def run_serve(args):
     the first 2..4 blocks of its test's exponent.  A first pass with every
     request arriving at once measures the service rate; the arrival rate is
     then 80 % of it."""
-    from genefer22_b200.autotune import Autotuner
     from genefer22_b200.serve import Server, serve_requests
     count = args.serve_requests
-    tuner = Autotuner(squarings=4, replays=2)
     sat = serve_requests(count, rate=1e9, blocks=[2, 3, 4], B=BLOCK, seed=1005)
-    srv = Server(B=BLOCK, budget_bytes=80 * 10**9, tuner=tuner)
+    srv = Server(B=BLOCK, budget_bytes=80 * 10**9)
     with Clocks(0) as ck0:
         srv.run(sat, timeout_s=1800)
     cap = srv.stats
     rate = 0.8 * cap.completed / cap.seconds
     reqs = serve_requests(count, rate=rate, blocks=[2, 3, 4], B=BLOCK, seed=1005)
-    srv = Server(B=BLOCK, budget_bytes=80 * 10**9, tuner=tuner)
+    srv = Server(B=BLOCK, budget_bytes=80 * 10**9)
     with Clocks(0) as ck:
         comps = srv.run(reqs, timeout_s=1800)
     st = srv.stats
@@ -484,7 +468,7 @@ def run_serve(args):
             "p50_time_to_residue_s": st.p50, "p99_time_to_residue_s": st.p99,
             "p50_time_to_validated_s": st.p50_validated, "p99_time_to_validated_s": st.p99_validated,
             "mean_queue_wait_s": st.mean_wait, "completed": st.completed, "gl_failures": st.gl_failures,
-            "pools_created": st.pools_created, "peak_budget_bytes": st.peak_bytes,
+            "pools_created": st.pools_created, "blocks_run": st.blocks_run, "peak_budget_bytes": st.peak_bytes,
             "saturated": {"value": cap.rate, "seconds": cap.seconds, "p50_s": cap.p50, "p99_s": cap.p99},
             "per_n": {str(k): v for k, v in st.per_n.items()},
             "clocks": ck.summary()}
@@ -532,21 +516,28 @@ def run_verify(args):
     print(json.dumps(line), flush=True)
 
 
-def run_sizes(args):
-    """Per size n = 12..23: a batch (tests per launch as in serving pools) run as
-    graph-replayed blocks vs the plain path (one test, one call per squaring)."""
+SIZE_TESTS = {12: 256, 13: 128, 14: 64, 15: 64, 16: 64, 17: 16, 18: 8, 19: 4, 20: 2, 21: 2, 22: 1, 23: 1}
+
+
+def w_min(b: int, n: int) -> int:
+    """RNS width the reference GPU transform picks (src/transform_ocl.cpp:35-50,
+    32-bit primes 125*2^25+1, 243*2^24+1): the W of the 16 W N roofline unit."""
+    return 2 if b * b < ((125 * 2**25 + 1) * (243 * 2**24 + 1) // 2) // (1 << n) else 3
+
+
+def size_rates(ns, tuner, rng, hbm):
+    """Per size n: a batch of SIZE_TESTS[n] tests (as in serving pools, plan
+    chosen by the autotuner) run as graph-replayed Gerbicz-Li blocks, against
+    the plain path (one test, one gfc_square_dup call per squaring); both as
+    digit-squarings/s, with the plain path's fraction of HBM roofline in the
+    16 W N bytes-per-squaring unit."""
     import torch
     from genefer22_b200 import Batch
     from genefer22_b200 import genefer as gf
-    from genefer22_b200.autotune import Autotuner
     from genefer22_b200.mixed import b_limit
-    torch.cuda.set_device(0)
-    tuner = Autotuner(squarings=4, replays=2)
-    rng = np.random.default_rng(11)
     out = {}
-    hbm, hbm_kind = peaks()
-    for n in range(12, 24):
-        count = {12: 256, 13: 128, 14: 64, 15: 64, 16: 64, 17: 16, 18: 8, 19: 4, 20: 2, 21: 2, 22: 1, 23: 1}[n]
+    for n in ns:
+        count = SIZE_TESTS[n]
         lim = min(b_limit(n), 100_000_000 if n >= 16 else 2_000_000_000)
         bs = [int(x) & ~1 for x in rng.integers(1_000_000, lim, size=count)]
         bt = Batch(bs, n, num_regs=3)
@@ -566,14 +557,76 @@ def run_sizes(args):
         sq_ms = ms / blk
         n_t, _ = plan_geometry(n, tr.lr)                  # packed plans: W = 4 planes of N/2
         alg_bytes = float(np.sum(16 * W * (1 << n_t)))
+        plain_us = (1 << n) / plain * 1e6
         out[n] = {"tests": count, "plan_lr": tr.lr, "widths": sorted(set(int(w) for w in W)),
                   "batched": batched, "plain": plain, "batched_over_plain": batched / plain,
-                  "us_per_batch_squaring": sq_ms * 1e3,
-                  "hbm_frac_16WN": alg_bytes / (sq_ms * 1e-3) / 1e9 / hbm}
+                  "us_per_batch_squaring": sq_ms * 1e3, "plain_us_per_squaring": plain_us,
+                  "hbm_frac_16WN": alg_bytes / (sq_ms * 1e-3) / 1e9 / hbm,
+                  "plain_hbm_frac_16WminN": 16 * w_min(bs[0], n) * (1 << n) / (plain_us * 1e-6) / 1e9 / hbm,
+                  "plain_b": bs[0]}
         g.close()
         bt.close()
+    return out
+
+
+def run_sizes(args):
+    """Per size n = 12..23: a batch (tests per launch as in serving pools) run as
+    graph-replayed blocks vs the plain path (one test, one call per squaring)."""
+    import torch
+    from genefer22_b200.autotune import Autotuner
+    torch.cuda.set_device(0)
+    hbm, hbm_kind = peaks()
+    out = size_rates(range(12, 24), Autotuner(squarings=4, replays=2), np.random.default_rng(11), hbm)
     print(json.dumps({"metric": METRIC, "unit": METRIC, "workload": "sizes", "hbm_peak_gbs": hbm,
                       "hbm_peak_kind": hbm_kind, "sizes": out}), flush=True)
+
+
+def north_star(args, bs):
+    """The north-star figures beside the default line, a few minutes in all:
+    the plain one-test path at n = 20 and 22 against the HBM roofline,
+    batched / plain for n = 16..22, a short serving pass (p50 / p99 time to
+    residue), and the reference's i32 transform (the same arithmetic, one
+    test per host core)."""
+    from genefer22_b200.autotune import Autotuner
+    from genefer22_b200.serve import Server, serve_requests
+    hbm, _ = peaks()
+    sz = size_rates(range(16, 23), Autotuner(squarings=4, replays=2), np.random.default_rng(11), hbm)
+    out = {"plain": {str(n): {"value": sz[n]["plain"], "us_per_squaring": sz[n]["plain_us_per_squaring"],
+                              "hbm_frac_16WminN": sz[n]["plain_hbm_frac_16WminN"], "b": sz[n]["plain_b"]}
+                     for n in (20, 22)},
+           "batched_over_plain": {str(n): sz[n]["batched_over_plain"] for n in sz},
+           "sizes": {str(n): {k: sz[n][k] for k in ("tests", "plan_lr", "batched", "plain", "us_per_batch_squaring")}
+                     for n in sz}}
+    reqs = serve_requests(args.serve_requests, rate=1e9, blocks=[2], B=BLOCK, seed=1005, ns=tuple(range(15, 21)),
+                          big=None)
+    srv = Server(B=BLOCK, budget_bytes=80 * 10**9)
+    srv.run(reqs, timeout_s=600)
+    st = srv.stats
+    out["serving"] = {"requests": st.completed, "arrivals": "all at t=0", "p50_time_to_residue_s": st.p50,
+                      "p99_time_to_residue_s": st.p99, "p99_time_to_validated_s": st.p99_validated,
+                      "value": st.rate, "gl_failures": st.gl_failures,
+                      "what": "native loop, n uniform 15..20, b even uniform up to the per-n limit, "
+                              "2 blocks of 1000 squarings each, seed 1005"}
+    try:
+        v, cores, sample, ttype = cpu_reference(N_LOG, bs, min(args.cpu_seconds, 8.0), impl="i32")
+        out["cpu_baseline_i32"] = {"value": v, "unit": METRIC, "cores": cores, "kind": "reference",
+                                   "sample": f"reference {ttype} transform (same integer arithmetic): {sample}"}
+    except Exception as e:          # reported, not fatal
+        out["cpu_baseline_i32"] = {"value": None, "sample": f"unavailable: {e}"}
+    return out
+
+
+def spawn_ranks(n: int) -> int:
+    """`python bench.py --gpus N` outside torchrun: the same command as N ranks,
+    one process per GPU (torch.distributed.run on 127.0.0.1, a free port),
+    so that the line reports N GPUs; returns the launcher's exit code."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -587,9 +640,12 @@ def main():
     ap.add_argument("--workload", default="batch", choices=["batch", "uneven", "serve", "sizes", "verify"],
                     help="batch: the default line; the others print their own line")
     ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--no-extras", action="store_true", help="skip the north-star block of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if (args.gpus > 1) and ("WORLD_SIZE" not in os.environ):
+        sys.exit(spawn_ranks(args.gpus))
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "uneven":

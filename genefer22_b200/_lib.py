@@ -21,8 +21,58 @@ vp = ctypes.c_void_p
 GFC_OK = 0
 ERRORS = {-1: "GFC_ERR_ARG", -2: "GFC_ERR_CUDA", -3: "GFC_ERR_RANGE", -4: "GFC_ERR_NUMERIC", -5: "GFC_ERR_STATE"}
 
+class ServerConfig(ctypes.Structure):
+    """gfc_server_config (include/gfcuda.h)."""
+    _fields_ = [("block", ctypes.c_uint32), ("validate_group", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64),
+                ("capacity", ctypes.c_uint32 * 24), ("device", ctypes.c_int32), ("tune", ctypes.c_int32),
+                ("keep_digits", ctypes.c_int32), ("idle_close_s", ctypes.c_double)]
+
+
+class CompletionC(ctypes.Structure):
+    """gfc_completion (include/gfcuda.h)."""
+    _fields_ = [("id", ctypes.c_uint64), ("nbits", ctypes.c_uint64), ("b", ctypes.c_uint32), ("n", ctypes.c_uint32),
+                ("arrival", ctypes.c_double), ("admitted", ctypes.c_double), ("residue_at", ctypes.c_double),
+                ("validated_at", ctypes.c_double), ("res64", ctypes.c_uint64), ("old64", ctypes.c_uint64),
+                ("is_prp", ctypes.c_int32), ("gl_ok", ctypes.c_int32), ("pool", ctypes.c_int32),
+                ("slot", ctypes.c_int32), ("plan", ctypes.c_int32)]
+
+
+class ServerStatsC(ctypes.Structure):
+    """gfc_server_stats (include/gfcuda.h)."""
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "completed", "pools_created", "pools_open", "blocks_run",
+                                               "used_bytes", "peak_bytes", "budget_bytes", "gl_failures")]
+
+
+# The serving loop's entry points (also exported by the CPU build of the same
+# loop that the host-logic tests load).
+SERVER_SIGNATURES = {
+    "gfc_server_default_config": (None, [ctypes.POINTER(ServerConfig)]),
+    "gfc_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+    "gfc_server_pretune": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_uint32]),
+    "gfc_server_submit": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, c_u32p, ctypes.c_uint64]),
+    "gfc_server_poll": (ctypes.c_int, [vp, ctypes.POINTER(CompletionC), ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_size_t), ctypes.c_int32]),
+    "gfc_server_digits": (ctypes.c_int, [vp, ctypes.c_uint64, c_i32p, ctypes.c_size_t]),
+    "gfc_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStatsC)]),
+    "gfc_server_clock": (ctypes.c_double, [vp]),
+    "gfc_server_destroy": (None, [vp]),
+    "gfc_server_slot_bytes": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64]),
+    "gfc_server_table_bytes": (ctypes.c_uint64, [ctypes.c_uint32]),
+    "gfc_server_default_capacity": (ctypes.c_uint32, [ctypes.c_uint32]),
+}
+
 # name: (restype, argtypes); every symbol declared in include/gfcuda.h
 SIGNATURES = {
+    **SERVER_SIGNATURES,
+    "gfc_batch_reserve": (ctypes.c_int, [vp, ctypes.c_uint64]),
+    "gfc_batch_admit": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_uint32, c_u32p, ctypes.c_uint64]),
+    "gfc_batch_get_async": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_size_t, c_i32p]),
+    "gfc_batch_set_async": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.c_size_t, c_i32p]),
+    "gfc_plan_candidates": (ctypes.c_int, [ctypes.c_uint32, c_i32p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "gfc_batch_tune": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_uint32, c_i32p, ctypes.POINTER(ctypes.c_float),
+                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), c_i32p]),
+    "gfc_width_for": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32]),
+    "gfc_packed_range": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32]),
     "gfc_last_error": (ctypes.c_char_p, []),
     "gfc_version": (ctypes.c_int, []),
     "gfc_create": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_size_t, ctypes.c_int, vp, ctypes.POINTER(vp)]),

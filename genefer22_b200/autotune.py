@@ -19,24 +19,25 @@ points instead of two or three on all of them.
 The reference has no counterpart: genefer runs one test per transform with a
 fixed GPU kernel split chosen from n (src/transformGPU.h:945-1083).
 
-The tuner captures K squarings of each candidate plan into a CUDA graph,
-replays it, and keeps the fastest (device time per squaring, taken as the
+The tuner is native (gfc_batch_tune, genefer22_b200/csrc/gf_host.cu): it
+captures K squarings of each candidate plan into a CUDA graph, replays it
+between CUDA events and keeps the fastest (device time per squaring, the
 minimum over a few replays).  It squares register 0 of the batch in place, so
-tune a batch before loading its tests.  Results are cached per
-(n, test count, tests on the 3-prime set) in memory and, optionally, in a JSON
-file.
+tune a batch before loading its tests.  This module caches the choice per
+(n, test count, tests on the 3-prime set, packed range) in memory and,
+optionally, in a JSON file.
 """
 from __future__ import annotations
 
+import ctypes
 import json
 import os
-import time
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
 
 import numpy as np
 
-from ._lib import GfcError
+from ._lib import GfcError, check, lib
 from .transform import Batch
 
 SMALL_MAX_LOGN = 14
@@ -48,39 +49,19 @@ PLAN_PACKED = 200
 PLAN_PACKED_SIX = 300
 
 
-# Prime set 2 of the engine (packed digits): the exact range of plans 200 + lr
-# and 300 + lr2 (the engine refuses other bases with GFC_ERR_RANGE).
-_P2 = (127 * 2**24 + 1, 63 * 2**25 + 1, 249 * 2**23 + 1, 15 * 2**27 + 1)
-_M2 = _P2[0] * _P2[1] * _P2[2] * _P2[3]
-
-
 def packed_ok(b: int, n: int) -> bool:
-    """Whether base b at size n fits packed digits (two per coefficient)."""
-    b = int(b)
-    return (1 << 20) <= b < (1 << 28) and ((b // 2 + 1) * (b + 1)) ** 2 < (_M2 // 2) // (1 << (int(n) - 1))
+    """Whether base b at size n fits packed digits (two per coefficient), the
+    range the engine enforces for plans 200 + lr and 300 + lr2 (gfc_packed_range)."""
+    return lib().gfc_packed_range(int(b), int(n)) == 1
 
 
 def candidates(n: int) -> List[int]:
-    """Plans the engine accepts for size n (it rejects the others with GFC_ERR_ARG)."""
-    out = [0] if n <= SMALL_MAX_LOGN else []
-    if 15 <= n <= 17:
-        out.append(PLAN_CLUSTER)
-    for lr in range(3, 11):
-        lc = n - lr
-        if 8 <= lc <= 13:
-            out.append(lr)
-    for lr in (3, 4):                       # packed digits: four primes, transform of N/2
-        if 8 <= n - 1 - lr <= 13:
-            out.append(PLAN_PACKED + lr)
-    for lr2 in range(3, 8):                 # packed digits, six-step on N/2
-        lc = n - 1 - 4 - lr2
-        if 8 <= lc <= 13 and max(32, 4096 >> lr2) <= (1 << lc):
-            out.append(PLAN_PACKED_SIX + lr2)
-    for lr2 in range(3, 8):                 # six-step: 2^4 x 2^lr2 column split
-        lc = n - 4 - lr2
-        if 8 <= lc <= 13 and max(32, 4096 >> lr2) <= (1 << lc):
-            out.append(PLAN_SIX + lr2)
-    return out
+    """Plans the engine accepts for size n (gfc_plan_candidates), in the order
+    the tuner measures them."""
+    out = (ctypes.c_int32 * 32)()
+    cnt = ctypes.c_size_t(0)
+    check(lib().gfc_plan_candidates(int(n), out, 32, ctypes.byref(cnt)))
+    return [int(out[i]) for i in range(cnt.value)]
 
 
 @dataclass
@@ -118,24 +99,6 @@ class Autotuner:
                 json.dump(self.cache, f, indent=1, sort_keys=True)
             os.replace(tmp, self.cache_path)
 
-    def measure(self, bt: Batch, lr: int) -> float:
-        """Microseconds per batch squaring of plan lr (graph replay, device-bound)."""
-        bt.set_plan(lr)
-        K = self.squarings
-        g = bt.capture(lambda: bt.square(False, K))
-        try:
-            g.launch()
-            bt.sync()
-            best = float("inf")
-            for _ in range(self.replays):
-                t0 = time.perf_counter()
-                g.launch()
-                bt.sync()
-                best = min(best, time.perf_counter() - t0)
-        finally:
-            g.close()
-        return best / K * 1e6
-
     def tune(self, bt: Batch, force: bool = False) -> TuneResult:
         """Chooses and sets the fastest plan for bt (before its tests are loaded)."""
         packable = all(packed_ok(b, bt.n) for b in bt.bases)
@@ -149,17 +112,14 @@ class Autotuner:
                                   packable)
             except GfcError:
                 pass                                  # a plan this batch cannot take: measure
-        us: Dict[int, float] = {}
-        for lr in candidates(bt.n):
-            try:
-                us[lr] = self.measure(bt, lr)
-            except GfcError:
-                continue
-        if not us:
-            raise GfcError(-1, f"no valid plan for n={bt.n}")
-        best = min(us, key=lambda lr: (us[lr], lr))
-        bt.set_plan(best)
-        bt.set(0)
+        plans = (ctypes.c_int32 * 32)()
+        times = (ctypes.c_float * 32)()
+        cnt = ctypes.c_size_t(0)
+        bestc = ctypes.c_int32(0)
+        check(lib().gfc_batch_tune(bt.handle, self.squarings, self.replays, plans, times, 32, ctypes.byref(cnt),
+                                   ctypes.byref(bestc)))
+        us: Dict[int, float] = {int(plans[i]): float(times[i]) for i in range(min(cnt.value, 32))}
+        best = int(bestc.value)
         self.cache[k] = {"lr": best, "us": {str(a): v for a, v in us.items()}}
         self._save()
         return TuneResult(bt.n, bt.count, wide, best, us, packable)

@@ -14,8 +14,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libgfcuda.so")
-SOURCES = [os.path.join(CSRC, "gf_host.cu"), os.path.join(CSRC, "gf_probe.cu"), os.path.join(CSRC, "gf_gint.cpp")]
-DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("gf_arith.cuh", "gf_ntt.cuh", "gf_kernels.cuh")] + \
+SOURCES = [os.path.join(CSRC, f) for f in ("gf_host.cu", "gf_probe.cu", "gf_gint.cpp", "gf_server.cpp",
+                                           "gf_server_cuda.cpp")]
+DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("gf_arith.cuh", "gf_ntt.cuh", "gf_kernels.cuh", "gf_server.h")] + \
     [os.path.join(ROOT, "include", "gfcuda.h")]
 
 NVCC_FLAGS = [

@@ -654,10 +654,22 @@ struct gfc_batch
 	int cluster_max = 0;          // clusters of k_cluster resident at once
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
+	// Reserved slots (gfc_batch_reserve): exponent words of every slot in one
+	// device buffer, and pinned host staging so that admission and the
+	// asynchronous register copies allocate nothing and never synchronise.
+	uint64_t res_bits = 0;        // exponent bits each slot can hold (0: not reserved)
+	size_t res_words = 0;         // device words per slot
+	uint32_t *d_eres = nullptr;   // count x res_words exponent words
+	char *h_pin = nullptr;        // pinned: per slot [TestDesc | int64 pos | res_words words], then tests[], one
+	size_t pin_slot = 0;          // bytes per slot in h_pin
+	std::vector<cudaEvent_t> slot_ev;   // recorded after a slot's staged copies were enqueued
 
 	~gfc_batch()
 	{
 		cudaSetDevice(device);
+		for (cudaEvent_t e : slot_ev) if (e != nullptr) cudaEventDestroy(e);
+		if (d_eres != nullptr) cudaFree(d_eres);
+		if (h_pin != nullptr) cudaFreeHost(h_pin);
 		for (uint32_t *e : ebits) if (e != nullptr) cudaFree(e);
 		if (mem != nullptr) cudaFree(mem);
 		if (own_stream && (stream != nullptr)) cudaStreamDestroy(stream);
@@ -1160,6 +1172,243 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 	return bt.release();
 }
 
+// ---- autotuner
+
+// Every plan the engine accepts at size n, in the order the tuner tries them:
+// single-CTA, cluster, four-step, packed four-step, packed six-step, six-step.
+std::vector<int> plan_candidates(int n)
+{
+	std::vector<int> out;
+	auto add = [&](int p) { if (plan_valid(n, p)) out.push_back(p); };
+	add(0);
+	add(PLAN_CLUSTER);
+	for (int lr = 3; lr <= 10; ++lr) add(lr);
+	for (int l = 3; l <= 4; ++l) add(PLAN_PACKED + l);
+	for (int l2 = 3; l2 <= 7; ++l2) add(PLAN_PACKED_SIX + l2);
+	for (int l2 = 3; l2 <= 7; ++l2) add(PLAN_SIX + l2);
+	return out;
+}
+
+void set_plan_checked(gfc_batch &bt, int lr);
+
+// Device time of one batch squaring under each candidate plan: `squarings`
+// squarings of register 0 captured into a CUDA graph, replayed `replays`
+// times between CUDA events on the batch stream, minimum taken.  Plans the
+// batch cannot take (a base outside the packed range) are skipped.  Sets the
+// fastest (ties: the lower code) and clears register 0.  Squares register 0 in
+// place: tune a batch before loading its tests.
+void op_tune(gfc_batch &bt, uint32_t squarings, uint32_t replays, int32_t *plans, float *us, size_t cap, size_t *count,
+			 int32_t *best)
+{
+	no_capture(bt);
+	const std::vector<int> cand = plan_candidates(bt.n);
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	GFC_CK(cudaEventCreate(&e0));
+	GFC_CK(cudaEventCreate(&e1));
+	std::vector<std::pair<int, float>> got;
+	try
+	{
+		for (int p : cand)
+		{
+			try { set_plan_checked(bt, p); }
+			catch (const Error &e) { if ((e.code == GFC_ERR_ARG) || (e.code == GFC_ERR_RANGE)) continue; throw; }
+			materialize(bt);
+			cudaGraph_t graph = nullptr;
+			cudaGraphExec_t exec = nullptr;
+			bt.capturing = true;
+			GFC_CK(cudaStreamBeginCapture(bt.stream, cudaStreamCaptureModeThreadLocal));
+			const uint64_t l0 = g_launches.load();
+			try
+			{
+				op_square(bt, DUP_NONE, squarings);
+				materialize(bt);
+			}
+			catch (...)
+			{
+				cudaStreamEndCapture(bt.stream, &graph);
+				if (graph != nullptr) cudaGraphDestroy(graph);
+				bt.capturing = false;
+				throw;
+			}
+			const uint64_t kernels = g_launches.load() - l0;
+			g_launches.fetch_sub(kernels);
+			bt.capturing = false;
+			GFC_CK(cudaStreamEndCapture(bt.stream, &graph));
+			float best_ms = 0;
+			try
+			{
+				GFC_CK(cudaGraphInstantiate(&exec, graph, 0));
+				GFC_CK(cudaGraphLaunch(exec, bt.stream));
+				g_launches.fetch_add(kernels);
+				for (uint32_t r = 0; r < replays; ++r)
+				{
+					GFC_CK(cudaEventRecord(e0, bt.stream));
+					GFC_CK(cudaGraphLaunch(exec, bt.stream));
+					g_launches.fetch_add(kernels);
+					GFC_CK(cudaEventRecord(e1, bt.stream));
+					GFC_CK(cudaEventSynchronize(e1));
+					float ms = 0;
+					GFC_CK(cudaEventElapsedTime(&ms, e0, e1));
+					if ((r == 0) || (ms < best_ms)) best_ms = ms;
+				}
+			}
+			catch (...)
+			{
+				if (exec != nullptr) cudaGraphExecDestroy(exec);
+				cudaGraphDestroy(graph);
+				throw;
+			}
+			cudaGraphExecDestroy(exec);
+			cudaGraphDestroy(graph);
+			got.emplace_back(p, 1000.0f * best_ms / static_cast<float>(squarings));
+		}
+	}
+	catch (...)
+	{
+		cudaEventDestroy(e0); cudaEventDestroy(e1);
+		throw;
+	}
+	cudaEventDestroy(e0); cudaEventDestroy(e1);
+	if (got.empty()) fail(GFC_ERR_RANGE, "tune: no plan accepts this batch");
+	size_t bi = 0;
+	for (size_t i = 1; i < got.size(); ++i)
+		if ((got[i].second < got[bi].second) || ((got[i].second == got[bi].second) && (got[i].first < got[bi].first))) bi = i;
+	set_plan_checked(bt, got[bi].first);
+	op_set(bt, 0);
+	GFC_CK(cudaStreamSynchronize(bt.stream));
+	for (size_t i = 0; (i < got.size()) && (i < cap); ++i)
+	{
+		if (plans != nullptr) plans[i] = got[i].first;
+		if (us != nullptr) us[i] = got[i].second;
+	}
+	*count = got.size();
+	*best = got[bi].first;
+}
+
+// ---- reserved slots: staged, asynchronous admission (gfc_batch_reserve)
+
+struct PinSlot
+{
+	TestDesc *desc;
+	int64_t *pos;
+	uint32_t *words;
+};
+
+PinSlot pin_slot(const gfc_batch &bt, size_t test)
+{
+	char *p = bt.h_pin + test * bt.pin_slot;
+	return { reinterpret_cast<TestDesc *>(p), reinterpret_cast<int64_t *>(p + sizeof(TestDesc)),
+			 reinterpret_cast<uint32_t *>(p + sizeof(TestDesc) + sizeof(int64_t)) };
+}
+
+int32_t *pin_tests(const gfc_batch &bt) { return reinterpret_cast<int32_t *>(bt.h_pin + bt.count * bt.pin_slot); }
+int32_t *pin_one(const gfc_batch &bt) { return pin_tests(bt) + bt.count; }
+
+void op_reserve(gfc_batch &bt, uint64_t max_bits)
+{
+	if (bt.res_bits != 0) fail(GFC_ERR_STATE, "reserve: the batch is already reserved");
+	if ((max_bits == 0) || (max_bits > (uint64_t(1) << 40))) fail(GFC_ERR_ARG, "reserve: need 1 <= max_bits <= 2^40");
+	no_capture(bt);
+	const size_t words = (((max_bits + 31) / 32) + 3) & ~size_t(3);        // 16-byte multiple per slot
+	const size_t slot = (sizeof(TestDesc) + sizeof(int64_t) + 4 * words + 15) & ~size_t(15);
+	GFC_CK(cudaMalloc(&bt.d_eres, bt.count * words * sizeof(uint32_t)));
+	GFC_CK(cudaMemsetAsync(bt.d_eres, 0, bt.count * words * sizeof(uint32_t), bt.stream));
+	void *h = nullptr;
+	GFC_CK(cudaHostAlloc(&h, bt.count * slot + (bt.count + 1) * sizeof(int32_t), cudaHostAllocDefault));
+	bt.h_pin = static_cast<char *>(h);
+	bt.res_words = words;
+	bt.pin_slot = slot;
+	*pin_one(bt) = 1;
+	bt.slot_ev.assign(bt.count + 1, nullptr);          // one per slot, then one for the tests list
+	for (cudaEvent_t &e : bt.slot_ev) GFC_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+	GFC_CK(cudaStreamSynchronize(bt.stream));
+	bt.res_bits = max_bits;
+}
+
+// Staging of slot `test` is rewritten only after its previous staged copies
+// ran (they ran long ago whenever the slot held a test for a block).
+void staging_free(gfc_batch &bt, size_t k) { GFC_CK(cudaEventSynchronize(bt.slot_ev[k])); }
+
+// Exponent of a reserved slot: words and position through the slot's pinned
+// staging, the descriptor's exponent pointer into the reserved buffer.
+void stage_exponent(gfc_batch &bt, size_t test, const uint32_t *words, uint64_t nbits)
+{
+	staging_free(bt, test);
+	const PinSlot ps = pin_slot(bt, test);
+	const size_t nw = (nbits + 31) / 32;
+	std::memcpy(ps.words, words, nw * sizeof(uint32_t));
+	TestDesc &d = bt.h_desc[test];
+	d.ebits = bt.d_eres + test * bt.res_words;
+	*ps.desc = d;
+	*ps.pos = static_cast<int64_t>(nbits) - 1;
+	GFC_CK(cudaMemcpyAsync(const_cast<uint32_t *>(d.ebits), ps.words, nw * sizeof(uint32_t), cudaMemcpyHostToDevice, bt.stream));
+	GFC_CK(cudaMemcpyAsync(bt.d_desc + test, ps.desc, sizeof(TestDesc), cudaMemcpyHostToDevice, bt.stream));
+	GFC_CK(cudaMemcpyAsync(bt.d_pos + test, ps.pos, sizeof(int64_t), cudaMemcpyHostToDevice, bt.stream));
+	GFC_CK(cudaEventRecord(bt.slot_ev[test], bt.stream));
+}
+
+// A new test in a reserved slot: base, r_0 = r_1 = 1, exponent, position;
+// everything enqueued on the batch stream.
+void op_admit(gfc_batch &bt, size_t test, uint32_t b, const uint32_t *words, uint64_t nbits)
+{
+	check_test(bt, test);
+	no_capture(bt);
+	if (bt.res_bits == 0) fail(GFC_ERR_STATE, "admit: reserve the batch first (gfc_batch_reserve)");
+	if ((nbits == 0) || (nbits > bt.res_bits)) fail(GFC_ERR_ARG, "admit: need 1 <= nbits <= the reserved bits");
+	if ((b < 8) || (b >= (1u << 31))) fail(GFC_ERR_ARG, "admit: base b must satisfy 8 <= b < 2^31");
+	const int s = choose_set(b, bt.n);
+	if (s < 0) fail(GFC_ERR_RANGE, "admit: (b, n) is outside the exact range of the RNS prime sets");
+	if (bt.packed && !packed_ok(b, bt.n)) fail(GFC_ERR_RANGE, "admit: base outside the range of packed digits");
+	materialize(bt);
+	if (s != bt.set[test])
+	{
+		// prime-set order of the per-set launches (single-CTA plan)
+		bt.sets_version++;
+		bt.nset[bt.set[test]]--;
+		bt.set[test] = s;
+		bt.nset[s]++;
+		bt.offset[0] = 0; bt.offset[1] = bt.nset[0];
+		staging_free(bt, bt.count);
+		int32_t *tl = pin_tests(bt);
+		size_t k = 0;
+		for (int q = 0; q < 2; ++q)
+			for (size_t i = 0; i < bt.count; ++i)
+				if (bt.set[i] == q) tl[k++] = static_cast<int32_t>(i);
+		GFC_CK(cudaMemcpyAsync(bt.d_tests, tl, bt.count * sizeof(int32_t), cudaMemcpyHostToDevice, bt.stream));
+		GFC_CK(cudaEventRecord(bt.slot_ev[bt.count], bt.stream));
+		if (bt.lr == 0) prepare_plan(bt);
+	}
+	bt.b[test] = b;
+	TestDesc &d = bt.h_desc[test];
+	d.b = b;
+	d.set = bt.packed ? 2 : s;
+	d.ck = carry_constants(b, bt.packed ? 1 : s);
+	if (bt.packed) d.pk = pack_constants(b);
+	// registers 0 and 1 (contiguous) = 1, no pending segment carries
+	int32_t *r = reg_ptr(bt, test, 0);
+	const size_t nr = (bt.num_regs >= 2) ? 2 : 1;
+	GFC_CK(cudaMemsetAsync(r, 0, nr * bt.N * sizeof(int32_t), bt.stream));
+	for (size_t k = 0; k < nr; ++k)
+		GFC_CK(cudaMemcpyAsync(r + k * bt.N, pin_one(bt), sizeof(int32_t), cudaMemcpyHostToDevice, bt.stream));
+	GFC_CK(cudaMemsetAsync(d.carry, 0, (bt.N / SEG) * PK_CARRY * sizeof(int64_t), bt.stream));
+	stage_exponent(bt, test, words, nbits);
+}
+
+void set_plan_checked(gfc_batch &bt, int lr)
+{
+	if (!plan_valid(bt.n, lr)) fail(GFC_ERR_ARG, "set_plan: invalid plan for this n");
+	const bool packed = lr > PLAN_PACKED;   // plans 200 + lr and 300 + lr2
+	if (packed)
+		for (size_t i = 0; i < bt.count; ++i)
+			if (!packed_ok(bt.b[i], bt.n)) fail(GFC_ERR_RANGE, "set_plan: a base is outside the range of packed digits");
+	no_capture(bt);
+	materialize(bt);                 // pending carries are in the current plan's format
+	GFC_CK(cudaStreamSynchronize(bt.stream));
+	if (packed != bt.packed) set_packed(bt, packed);
+	apply_plan(bt, lr);
+	prepare_plan(bt);
+}
+
 template <class F>
 int guard(F &&f)
 {
@@ -1188,6 +1437,10 @@ int guard(F &&f)
 // ------------------------------------------------------------------ C ABI
 
 #define GFC_API extern "C" __attribute__((visibility("default")))
+
+// The message gfc_last_error returns on this thread, for the other sources of
+// the library (gf_server_cuda.cpp).
+void gfc_internal_set_error(const char *msg) { g_err = (msg != nullptr) ? msg : ""; }
 
 GFC_API const char *gfc_last_error(void) { return g_err.c_str(); }
 GFC_API int gfc_version(void) { return 100; }
@@ -1344,6 +1597,11 @@ GFC_API int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *w
 		no_capture(*bt);
 		if (nbits == 0) fail(GFC_ERR_ARG, "set_exponent: empty exponent");
 		cudaSetDevice(bt->device);
+		if ((bt->res_bits != 0) && (nbits <= bt->res_bits))
+		{
+			stage_exponent(*bt, test, words, nbits);
+			return;
+		}
 		GFC_CK(cudaStreamSynchronize(bt->stream));
 		const size_t nw = (nbits + 31) / 32;
 		if (bt->ebits[test] != nullptr) { GFC_CK(cudaFree(bt->ebits[test])); bt->ebits[test] = nullptr; }
@@ -1353,6 +1611,80 @@ GFC_API int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *w
 		GFC_CK(cudaMemcpy(bt->d_desc + test, &bt->h_desc[test], sizeof(TestDesc), cudaMemcpyHostToDevice));
 		const int64_t pos = static_cast<int64_t>(nbits) - 1;
 		GFC_CK(cudaMemcpy(bt->d_pos + test, &pos, sizeof(pos), cudaMemcpyHostToDevice));
+	});
+}
+
+GFC_API int gfc_batch_reserve(gfc_batch *bt, uint64_t max_bits)
+{
+	return guard([&] { GFC_NULLCHK(bt); cudaSetDevice(bt->device); op_reserve(*bt, max_bits); });
+}
+
+GFC_API int gfc_batch_admit(gfc_batch *bt, size_t test, uint32_t b, const uint32_t *words, uint64_t nbits)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(words);
+		cudaSetDevice(bt->device);
+		op_admit(*bt, test, b, words, nbits);
+	});
+}
+
+GFC_API int gfc_batch_get_async(gfc_batch *bt, size_t test, size_t reg, int32_t *out)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(out);
+		check_test(*bt, test); check_reg(*bt, reg);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		materialize(*bt);
+		GFC_CK(cudaMemcpyAsync(out, reg_ptr(*bt, test, reg), bt->N * sizeof(int32_t), cudaMemcpyDeviceToHost, bt->stream));
+	});
+}
+
+GFC_API int gfc_batch_set_async(gfc_batch *bt, size_t test, size_t reg, const int32_t *in)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(in);
+		check_test(*bt, test); check_reg(*bt, reg);
+		check_digits(*bt, test, in);
+		no_capture(*bt);
+		cudaSetDevice(bt->device);
+		materialize(*bt);
+		GFC_CK(cudaMemcpyAsync(reg_ptr(*bt, test, reg), in, bt->N * sizeof(int32_t), cudaMemcpyHostToDevice, bt->stream));
+	});
+}
+
+GFC_API int gfc_width_for(uint32_t b, uint32_t n)
+{
+	if ((b < 8) || (b >= (1u << 31)) || (n < 8) || (n > 23)) return GFC_ERR_ARG;
+	const int s = choose_set(b, static_cast<int>(n));
+	return (s < 0) ? GFC_ERR_RANGE : ((s == 0) ? 2 : 3);
+}
+
+GFC_API int gfc_packed_range(uint32_t b, uint32_t n)
+{
+	if ((n < 9) || (n > 23)) return 0;
+	return packed_ok(b, static_cast<int>(n)) ? 1 : 0;
+}
+
+GFC_API int gfc_plan_candidates(uint32_t n, int32_t *plans, size_t cap, size_t *count)
+{
+	return guard([&] {
+		GFC_NULLCHK(count);
+		const std::vector<int> c = plan_candidates(static_cast<int>(n));
+		if ((plans == nullptr) && (cap != 0)) fail(GFC_ERR_ARG, "plan_candidates: null output");
+		for (size_t i = 0; (i < c.size()) && (i < cap); ++i) plans[i] = c[i];
+		*count = c.size();
+	});
+}
+
+GFC_API int gfc_batch_tune(gfc_batch *bt, uint32_t squarings, uint32_t replays, int32_t *plans, float *us, size_t cap,
+						   size_t *count, int32_t *best)
+{
+	return guard([&] {
+		GFC_NULLCHK(bt); GFC_NULLCHK(count); GFC_NULLCHK(best);
+		if ((squarings == 0) || (replays == 0)) fail(GFC_ERR_ARG, "tune: need squarings >= 1 and replays >= 1");
+		cudaSetDevice(bt->device);
+		op_tune(*bt, squarings, replays, plans, us, cap, count, best);
 	});
 }
 
@@ -1402,7 +1734,7 @@ GFC_API int gfc_batch_set_pos(gfc_batch *bt, const int64_t *pos)
 		no_capture(*bt);
 		cudaSetDevice(bt->device);
 		for (size_t i = 0; i < bt->count; ++i)
-			if ((pos[i] >= 0) && (bt->ebits[i] == nullptr)) fail(GFC_ERR_STATE, "set_pos: test has no exponent");
+			if ((pos[i] >= 0) && (bt->h_desc[i].ebits == nullptr)) fail(GFC_ERR_STATE, "set_pos: test has no exponent");
 		GFC_CK(cudaMemcpyAsync(bt->d_pos, pos, bt->count * sizeof(int64_t), cudaMemcpyHostToDevice, bt->stream));
 		GFC_CK(cudaStreamSynchronize(bt->stream));
 	});
@@ -1510,18 +1842,8 @@ GFC_API int gfc_batch_set_plan(gfc_batch *bt, int lr)
 {
 	return guard([&] {
 		GFC_NULLCHK(bt);
-		if (!plan_valid(bt->n, lr)) fail(GFC_ERR_ARG, "set_plan: invalid plan for this n");
-		const bool packed = lr > PLAN_PACKED;   // plans 200 + lr and 300 + lr2
-		if (packed)
-			for (size_t i = 0; i < bt->count; ++i)
-				if (!packed_ok(bt->b[i], bt->n)) fail(GFC_ERR_RANGE, "set_plan: a base is outside the range of packed digits");
-		no_capture(*bt);
 		cudaSetDevice(bt->device);
-		materialize(*bt);                 // pending carries are in the current plan's format
-		GFC_CK(cudaStreamSynchronize(bt->stream));
-		if (packed != bt->packed) set_packed(*bt, packed);
-		apply_plan(*bt, lr);
-		prepare_plan(*bt);
+		set_plan_checked(*bt, lr);
 	});
 }
 

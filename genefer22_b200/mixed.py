@@ -1,37 +1,32 @@
 """Uneven batches: tests of different sizes n in flight together.
 
-Tests are grouped into size classes (one ``Batch`` per n, its plan chosen by
-the ``Autotuner``); every class has its own CUDA stream and replays one graph
-per Gerbicz-Li block, and the host enqueues the classes' blocks round-robin,
-so the classes' launches overlap on the device.  A test's arithmetic depends
-only on its own registers, base and exponent bits, so its residue is the same
-alone and in the mix; ``run_alone`` computes it alone for that comparison.
+The native request loop (``gfc_server_*``, genefer22_b200/csrc/gf_server.cpp)
+schedules them: every test is submitted at once, each size class gets one
+pool with a slot per test (its plan chosen by the native autotuner), and the
+dispatcher thread launches every class's Gerbicz-Li block as a CUDA graph on
+the class's own stream as soon as its previous block is done, so the
+classes' launches overlap on the device.  Finished tests are read back and
+checked (genefer's Gerbicz-Li check, src/genefer.h:557-615) by the same loop.
+A test's arithmetic depends only on its own slot, base and exponent bits, so
+its residue is the same alone and in the mix; ``run_alone`` computes it
+alone for that comparison.
 
 The reference runs one test per process (src/genefer.h:1360-1480); mixing
 sizes has no counterpart there.
 """
 from __future__ import annotations
 
-import time
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
 from . import gint
-from .autotune import Autotuner, TuneResult
+from .autotune import Autotuner
+from .exponent import B_GerbiczLi
 from .genefer import BatchPRP, Job, Result
+from .serve import Request, Server
 from .transform import Batch
-
-
-@dataclass
-class SizeClass:
-    n: int
-    index: List[int]                 # positions of the class's tests in the job list
-    batch: Batch
-    prp: BatchPRP
-    tune: Optional[TuneResult] = None
-    blocks: List[int] = field(default_factory=list)
 
 
 @dataclass
@@ -46,33 +41,28 @@ class MixedStats:
 
 
 class MixedBatch:
-    """Runs ``jobs`` (any mix of n) with one Batch and graph per size class.
+    """Runs ``jobs`` (any mix of n): one pool per size class, a slot per test.
 
-    B: Gerbicz-Li block length, an int for every class, or None for genefer's
-    B_GerbiczLi of each class's longest exponent (src/genefer.h:467-471).
+    B: Gerbicz-Li block length shared by the classes, or None for genefer's
+    B_GerbiczLi of the longest exponent (src/genefer.h:467-471); tuner: any
+    Autotuner turns the native plan tuning on (None keeps the default plans).
     """
 
     def __init__(self, jobs: Sequence[Job], B: Optional[int] = None, tuner: Optional[Autotuner] = None,
                  device: int = 0, num_regs: int = 3):
         self.jobs = list(jobs)
         self.device = device
-        self.classes: List[SizeClass] = []
-        by_n: Dict[int, List[int]] = {}
-        for i, j in enumerate(self.jobs):
-            by_n.setdefault(int(j.n), []).append(i)
-        for n in sorted(by_n):
-            idx = by_n[n]
-            bt = Batch([self.jobs[i].b for i in idx], n, num_regs=num_regs, device=device)
-            tr = tuner.tune(bt) if tuner is not None else None
-            exps = [(self.jobs[i].words, self.jobs[i].nbits) for i in idx]
-            prp = BatchPRP(bt, B, exps=exps)
-            self.classes.append(SizeClass(n, idx, bt, prp, tr, prp.schedule()))
+        self.B = int(B) if B else B_GerbiczLi(max(int(j.nbits) for j in self.jobs))
+        self.tune = tuner is not None
+        self.counts: Dict[int, int] = {}
+        for j in self.jobs:
+            self.counts[int(j.n)] = self.counts.get(int(j.n), 0) + 1
+        self._canon: List[Optional[np.ndarray]] = [None] * len(self.jobs)
+        self._plans: Dict[int, int] = {}
+        self.stats = MixedStats()
 
     def close(self):
-        for c in self.classes:
-            c.prp._graph = None
-            c.batch.close()
-        self.classes = []
+        pass
 
     def __enter__(self):
         return self
@@ -81,56 +71,33 @@ class MixedBatch:
         self.close()
 
     def plans(self) -> Dict[int, int]:
-        return {c.n: c.batch.plan() for c in self.classes}
+        """Plan of each size class's pool (after ``run``)."""
+        return dict(self._plans)
 
     def run(self, validate: bool = True) -> List[Result]:
         """Runs every test to the end of its exponent; results in job order."""
-        for c in self.classes:
-            c.prp.load()
-        for c in self.classes:            # record the graphs before timing anything
-            if len(c.blocks) > 1:
-                c.prp.block_graph()
-        t0 = time.perf_counter()
-        step = 0
-        left = True
-        while left:
-            left = False
-            for c in self.classes:
-                if step >= len(c.blocks):
-                    continue
-                left = True
-                cnt = c.blocks[step]
-                if step == len(c.blocks) - 1:
-                    c.batch.square_exp(cnt)
-                elif cnt == c.prp.B:
-                    c.prp.block_graph().launch()
-                else:
-                    c.batch.square_exp(cnt)
-                    c.batch.gl_step()
-            step += 1
-        done = {}
-        for c in self.classes:
-            c.batch.sync()
-            done[c.n] = time.perf_counter() - t0
-        self.stats = MixedStats(seconds=max(done.values()) if done else 0.0)
-        for c in self.classes:
-            ds = float(sum(self.jobs[i].nbits for i in c.index)) * (1 << c.n)
-            self.stats.digit_squarings += ds
-            self.stats.per_class[c.n] = {"tests": len(c.index), "plan": c.batch.plan(), "B": c.prp.B,
-                                         "blocks": len(c.blocks), "digit_squarings": ds, "synced_at_s": done[c.n]}
-        out: List[Optional[Result]] = [None] * len(self.jobs)
-        for c in self.classes:
-            for k, r in zip(c.index, c.prp.results(validate)):
-                out[k] = r
-        return out                          # type: ignore[return-value]
+        srv = Server(B=self.B, capacity=lambda n: self.counts.get(n, 1), tune=self.tune, validate=validate,
+                     validate_group=4, keep_digits=True, device=self.device, idle_close_s=60.0)
+        comps = srv.run([Request(i, j, 0.0) for i, j in enumerate(self.jobs)])
+        st = srv.stats
+        self.stats = MixedStats(seconds=max(c.residue_at for c in comps) - min(c.arrival for c in comps),
+                                digit_squarings=float(sum((1 << j.n) * j.nbits for j in self.jobs)))
+        out: List[Result] = []
+        for i, (j, c) in enumerate(zip(self.jobs, comps)):
+            self._canon[i] = c.digits
+            self._plans[int(j.n)] = c.plan
+            out.append(Result(int(j.b), int(j.n), c.is_prp, c.res64, c.old64, True if c.gl_ok is None else c.gl_ok))
+        for n, k in sorted(self.counts.items()):
+            sub = [c for c in comps if c.n == n]
+            self.stats.per_class[n] = {"tests": k, "plan": self._plans.get(n), "B": self.B,
+                                       "digit_squarings": float(sum((1 << n) * c.nbits for c in sub)),
+                                       "residue_at_s": max(c.residue_at for c in sub)}
+        self.server_stats = st
+        return out
 
     def residues(self) -> List[np.ndarray]:
         """Canonical digits of every test's residue (after ``run``), in job order."""
-        out: List[Optional[np.ndarray]] = [None] * len(self.jobs)
-        for c in self.classes:
-            for k, i in enumerate(c.index):
-                out[i] = c.prp.canon[k]
-        return out                          # type: ignore[return-value]
+        return list(self._canon)                # type: ignore[return-value]
 
 
 def run_alone(job: Job, B: int, device: int = 0, plan: Optional[int] = None):

@@ -11,6 +11,7 @@ import argparse
 
 import numpy as np
 
+from ._lib import lib
 from .transform import Batch
 
 
@@ -22,6 +23,8 @@ def main():
     ap.add_argument("--plan", type=int, default=-1, help="-1: the default plan")
     ap.add_argument("--squarings", type=int, default=2)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--read", action="store_true", help="read register 0 back at the end (carry fix-up kernel)")
+    ap.add_argument("--mulscalar", type=int, default=0, help="then squareMul by this a (|a| > 2: k_mulscalar)")
     a = ap.parse_args()
     rng = np.random.default_rng(a.seed)
     bases = [int(x) & ~1 for x in rng.integers(1_000_000, a.bmax, size=a.count)]
@@ -31,6 +34,13 @@ def main():
         for i, b in enumerate(bases):
             bt.put(i, rng.integers(-(b // 2), b // 2, size=1 << a.n, dtype=np.int64).astype(np.int32))
         bt.square(False, a.squarings)
+        if a.mulscalar:
+            # gfc_square_mul on the batch handle: every test squared, then times a
+            rc = lib().gfc_square_mul(bt.handle, a.mulscalar)
+            if rc != 0:
+                raise RuntimeError(lib().gfc_last_error().decode())
+        if a.read:
+            bt.get(0, 0)
         bt.sync()
         print(f"n={a.n} tests={a.count} plan={bt.plan()} widths={sorted(set(bt.widths().tolist()))} squarings={a.squarings}")
 

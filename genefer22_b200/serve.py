@@ -1,72 +1,90 @@
-"""Serving: a request loop with continuous batching on one GPU.
+"""Serving: continuous batching on one GPU, run by the native request loop.
 
-Requests (a PRP test, or the first k squarings of one: ``Job``) arrive over
-time.  Tests of one size n share a *pool*: a ``Batch`` of ``capacity`` slots
-with its own CUDA stream and host thread, whose CUDA graph runs one
-Gerbicz-Li block for every slot:
+The loop is libgfcuda.so's ``gfc_server_*`` (genefer22_b200/csrc/gf_server.cpp):
+a dispatcher thread keeps one pool of slots per size n, each pool a batch
+whose Gerbicz-Li block (the d(t) update of src/genefer.h:529-535, then B
+squarings with each slot's own exponent bits) is one CUDA graph replay.
+Between two blocks of a pool, finished tests are read back and waiting tests
+of that size enter free slots without any allocation or synchronisation, so
+requests that arrive while others run are admitted as slots and memory free
+up and the pools' blocks overlap on the device.  Pools open while the
+device-memory budget allows and close when idle.  Finished tests get
+genefer's Gerbicz-Li check (src/genefer.h:557-615), several of one size at
+once, on a checker batch of their own.
 
-    d <- d * x   (the d(t) update of src/genefer.h:529-535)
-    B squarings of x, exponent bits taken per slot from its own position
-
-A slot that holds no test, or whose test has run out of exponent bits, sits
-out the squarings (its position is below 0).  A new test enters a free slot
-between two blocks with x = d = 1, so the d update that opens its first block
-leaves d = 1, as genefer starts (src/genefer.h:492-497); its exponent is
-padded with leading zero bits to a whole number of blocks.  When a test's
-last block ends, its x and d(t) are read back, the residue is reported
-(``residue_at``), the slot is freed, and x and d(t) go to the validator
-thread of that size, which runs genefer's Gerbicz-Li check
-(src/genefer.h:557-615) for several finished tests at once on a batch of its
-own (``validated_at``).
-
-Pools are created while the device-memory budget allows (per slot:
-registers, transform planes, multiplicand, carries and room for the longest
-exponent of its size; per size: the root tables) and closed after a short idle time, which returns their memory
-to the budget.  Requests wait in a per-size queue until a slot is free.
-
-Every test's arithmetic reads only its own slot, base and exponent bits, so a
-residue is the same whether the test ran alone or among others; tests check
-this against ``mixed.run_alone``.
+This module is the thin Python driver: it submits each request at its
+arrival time, collects the completions and summarises them (time to residue
+p50 / p99, digit-squarings per second).  Every test's arithmetic reads only
+its own slot, base and exponent bits, so a residue is the same whether the
+test ran alone or among others; tests check this against ``mixed.run_alone``.
 
 The reference has no counterpart: genefer runs one test per process
 (src/genefer.h:1360-1480).
 """
 from __future__ import annotations
 
-import collections
-import threading
+import ctypes
 import time
 from dataclasses import dataclass, field
-from typing import Deque, Dict, List, Optional, Sequence
+from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
 
-from . import gint
-from .autotune import Autotuner, packed_ok
-from .exponent import chunk_sum
-from .genefer import Job, gl_validate
-from .transform import Batch
+from ._lib import GFC_OK, SERVER_SIGNATURES, CompletionC, GfcError, ServerConfig, ServerStatsC, lib
+from .autotune import packed_ok
+from .genefer import Job
 
 NUM_REGS = 3
+MAX_N = 23
 
 
-def slot_bytes(n: int, num_regs: int = NUM_REGS) -> int:
-    """Device bytes of one batch slot of size n: registers, 3 transform planes,
-    3 multiplicand planes, segment carries, descriptor and position."""
-    N = 1 << int(n)
-    return num_regs * 4 * N + 12 * N + 12 * N + (N // 16) * 8 + 256
+vp = ctypes.c_void_p
+
+
+def bind(L):
+    """Sets the gfc_server_* signatures on a loaded library (libgfcuda.so, or
+    the CPU build of the same loop the host-logic tests use)."""
+    for name, (res, args) in {**SERVER_SIGNATURES, "gfc_last_error": (ctypes.c_char_p, [])}.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+_bound = None
+
+
+def _default_lib():
+    global _bound
+    if _bound is None:
+        _bound = bind(lib())
+    return _bound
+
+
+def slot_bytes(n: int, max_bits: int = 0) -> int:
+    """Device bytes of one pool slot of size n (registers, transform planes,
+    multiplicand, segment carries, descriptor) plus an exponent of max_bits."""
+    return int(_default_lib().gfc_server_slot_bytes(int(n), int(max_bits)))
 
 
 def table_bytes(n: int) -> int:
-    """Root tables of size n, shared by every batch of that size on a device:
-    the two 32-bit primes at one word per root, the three 31-bit primes at two
-    (root and Shoup quotient), forward and inverse (16 N words), and the four
-    primes of packed digits on N/2 points at two words per root (8 N words)."""
-    return 24 * 4 * (1 << int(n))
+    """Root tables of size n, counted once per size while a pool of it is open."""
+    return int(_default_lib().gfc_server_table_bytes(int(n)))
 
 
-def exponent_bytes(nbits: int) -> int:
-    return 4 * ((int(nbits) + 31) // 32) + 256
+def default_capacity(n: int) -> int:
+    """Slots per pool: enough tests per launch to fill the GPU at small n,
+    few at large n where one test already fills it."""
+    return int(_default_lib().gfc_server_default_capacity(int(n)))
+
+
+# From this size a pool opened for a base in the packed-digit range takes only
+# such bases (the native loop's rule, gfs::Devices::packed_pool_min_n).
+PACKED_POOL_MIN_N = 19
+
+
+def _packed_pool(b: int, n: int) -> bool:
+    return (int(n) >= PACKED_POOL_MIN_N) and packed_ok(b, n)
 
 
 @dataclass
@@ -82,7 +100,7 @@ class Completion:
     b: int
     n: int
     nbits: int
-    arrival: float
+    arrival: float                  # seconds after the start of the run (all times below too)
     admitted: float = 0.0
     residue_at: float = 0.0
     validated_at: Optional[float] = None
@@ -92,157 +110,13 @@ class Completion:
     gl_ok: Optional[bool] = None
     pool: int = -1
     slot: int = -1
+    plan: int = -1
     digits: Optional[np.ndarray] = None
 
     @property
     def latency(self) -> float:
         """Time to residue: arrival to the residue read back."""
         return self.residue_at - self.arrival
-
-
-@dataclass
-class _Active:
-    req: Request
-    comp: Completion
-    blocks_left: int
-
-
-def default_capacity(n: int) -> int:
-    """Slots per pool: enough tests per launch to fill the GPU at small n,
-    few at large n where one test already fills it."""
-    return {15: 32, 16: 32, 17: 16, 18: 8, 19: 4, 20: 2, 21: 2, 22: 1, 23: 1}.get(int(n), 32 if n < 15 else 1)
-
-
-class _Budget:
-    def __init__(self, limit: int):
-        self.limit = int(limit)
-        self.used = 0
-        self.peak = 0
-        self.tables: Dict[int, int] = {}       # n -> pools holding the tables
-
-    def need(self, n: int, nbytes: int) -> int:
-        return nbytes + (0 if self.tables.get(n, 0) > 0 else table_bytes(n))
-
-    def take(self, n: int, nbytes: int) -> bool:
-        total = self.need(n, nbytes)
-        if self.used + total > self.limit:
-            return False
-        self.used += total
-        self.peak = max(self.peak, self.used)
-        self.tables[n] = self.tables.get(n, 0) + 1
-        return True
-
-    def give(self, n: int, nbytes: int):
-        self.tables[n] -= 1
-        self.used -= nbytes + (table_bytes(n) if self.tables[n] == 0 else 0)
-
-
-# From this size, packed digits are faster even for pools of one or two tests
-# (measured); smaller sizes keep one kind of pool, so that requests are not
-# split between two half-full pools.
-PACKED_POOL_MIN_N = 19
-
-
-def _packed_pool(b: int, n: int) -> bool:
-    return (int(n) >= PACKED_POOL_MIN_N) and packed_ok(b, n)
-
-
-class _Pool:
-    """Slots of one size.  A pool opened (at n >= PACKED_POOL_MIN_N) for a base
-    in the packed range tunes with that base, so that packed plans are
-    candidates, and takes only such bases; any other pool takes every base."""
-
-    def __init__(self, server: "Server", pid: int, n: int, capacity: int, nbytes: int, rep_b: int = 1024):
-        self.server, self.pid, self.n, self.capacity, self.nbytes = server, pid, n, capacity, nbytes
-        self.rep_b = int(rep_b)
-        self.packed_only = _packed_pool(rep_b, n)
-        self.slots: List[Optional[_Active]] = [None] * capacity
-        self.reserved = 0                       # admitted by the dispatcher, not yet loaded
-        self.batch: Optional[Batch] = None
-        self.graph = None
-        self.plan = -1
-        self.blocks_run = 0
-        self.thread = threading.Thread(target=self._main, name=f"pool{pid}-n{n}", daemon=True)
-
-    def free_slots(self) -> int:
-        return self.capacity - sum(s is not None for s in self.slots) - self.reserved
-
-    # -- runs on the pool's thread
-    def _setup(self):
-        srv = self.server
-        self.batch = Batch([self.rep_b] * self.capacity, self.n, num_regs=NUM_REGS, device=srv.device)
-        if srv.tuner is not None:
-            self.plan = srv.tuner.tune(self.batch).lr
-        else:
-            self.plan = self.batch.plan()
-        bt, B = self.batch, srv.B
-        self.graph = bt.capture(lambda: (bt.gl_step(), bt.square_exp(B)))
-        self.one = np.zeros(1 << self.n, dtype=np.int32)
-        self.one[0] = 1
-
-    def _load(self, slot: int, act: _Active):
-        bt, B = self.batch, self.server.B
-        job = act.req.job
-        nb_pad = ((job.nbits + B - 1) // B) * B
-        words = np.zeros((nb_pad + 31) // 32, dtype=np.uint32)
-        words[: job.words.size] = job.words
-        bt.assign(slot, job.b)
-        bt.put(slot, self.one, 0)
-        bt.put(slot, self.one, 1)
-        bt.set_exponent(slot, words, nb_pad)
-        act.blocks_left = nb_pad // B
-
-    def _retire(self, slot: int, act: _Active):
-        bt = self.batch
-        x = bt.get(slot, 0)
-        d = bt.get(slot, 1)
-        c = act.comp
-        canon = gint.unbalance(x, c.b)
-        c.is_prp, c.res64, c.old64 = gint.is_one(canon, c.b)
-        c.residue_at = self.server.clock()
-        if self.server.keep_digits:
-            c.digits = canon
-        self.server._finished(self, slot, act, x, d)
-
-    def _main(self):
-        srv = self.server
-        try:
-            self._setup()
-            idle_since = srv.clock()
-            while True:
-                with srv.cv:
-                    new = srv._take_for(self)
-                for slot, act in new:
-                    self._load(slot, act)
-                    with srv.cv:
-                        self.slots[slot] = act
-                        self.reserved -= 1
-                if not any(s is not None for s in self.slots):
-                    with srv.cv:
-                        if srv._pool_should_close(self, idle_since):
-                            srv._close_pool(self)
-                            break
-                        srv.cv.wait(0.002)
-                    continue
-                self.graph.launch()
-                self.batch.sync()
-                self.blocks_run += 1
-                for slot, act in enumerate(self.slots):
-                    if act is None:
-                        continue
-                    act.blocks_left -= 1
-                    if act.blocks_left == 0:
-                        self._retire(slot, act)
-                idle_since = srv.clock()
-        except BaseException as e:            # surfaced by Server.run
-            with srv.cv:
-                srv.errors.append(e)
-                srv._close_pool(self)
-        finally:
-            self.graph = None
-            if self.batch is not None:
-                self.batch.close()
-                self.batch = None
 
 
 @dataclass
@@ -257,6 +131,7 @@ class ServeStats:
     p99_validated: float = 0.0
     mean_wait: float = 0.0
     pools_created: int = 0
+    blocks_run: int = 0
     peak_bytes: int = 0
     budget_bytes: int = 0
     gl_failures: int = 0
@@ -268,250 +143,120 @@ class ServeStats:
 
 
 class Server:
-    """Continuous-batching request loop on one device.
+    """Driver of the native continuous-batching loop on one device.
 
     B: Gerbicz-Li block length shared by every pool; capacity(n): slots per
-    pool; budget_bytes: device memory that pools and validators may hold.
+    pool; budget_bytes: device memory that pools and checkers may hold;
+    tune: autotune each pool shape's plan (before the clock starts);
+    validate_group: finished tests checked together (validate=False: none);
+    lib: a library exporting the gfc_server_* ABI (default libgfcuda.so).
     """
 
-    def __init__(self, B: int = 1000, budget_bytes: int = 80 * 10**9, capacity=default_capacity,
-                 tuner: Optional[Autotuner] = None, validate: bool = True, validate_group: int = 4,
-                 keep_digits: bool = False, device: int = 0, idle_close_s: float = 0.25):
+    def __init__(self, B: int = 1000, budget_bytes: int = 80 * 10**9,
+                 capacity: Optional[Callable[[int], int]] = None, tune: bool = True, validate: bool = True,
+                 validate_group: int = 4, keep_digits: bool = False, device: int = 0, idle_close_s: float = 0.25,
+                 lib=None):
         self.B = int(B)
-        self.budget = _Budget(budget_bytes)
+        self.budget_bytes = int(budget_bytes)
         self.capacity = capacity
-        self.tuner = tuner
-        self.validate = validate
-        self.validate_group = int(validate_group)
-        self.keep_digits = keep_digits
-        self.device = device
-        self.idle_close_s = idle_close_s
-        self.cv = threading.Condition()
-        self.errors: List[BaseException] = []
+        self.tune = bool(tune)
+        self.validate = bool(validate)
+        self.validate_group = int(validate_group) if validate else 0
+        self.keep_digits = bool(keep_digits)
+        self.device = int(device)
+        self.idle_close_s = float(idle_close_s)
+        self.L = bind(lib) if lib is not None else _default_lib()
+        self.stats = ServeStats()
 
-    # ---------------------------------------------------------------- clock
-    def clock(self) -> float:
-        return time.perf_counter() - self._t0
+    def _check(self, rc: int):
+        if rc != GFC_OK:
+            raise GfcError(rc, self.L.gfc_last_error().decode(errors="replace"))
 
-    # ------------------------------------------------------ called under cv
-    def _take_for(self, pool: _Pool):
-        """Moves waiting requests of the pool's size into its free slots."""
-        q = self.waiting[pool.n]
-        out = []
-        for slot in range(pool.capacity):
-            if pool.slots[slot] is not None:
-                continue
-            req = next((r for r in q if not pool.packed_only or _packed_pool(r.job.b, pool.n)), None)
-            if req is None:
-                break
-            q.remove(req)
-            pool.reserved += 1
-            c = Completion(req.id, req.job.b, req.job.n, req.job.nbits, req.arrival, admitted=self.clock(),
-                           pool=pool.pid, slot=slot)
-            out.append((slot, _Active(req, c, 0)))
-        return out
+    def _config(self) -> ServerConfig:
+        cfg = ServerConfig()
+        self.L.gfc_server_default_config(ctypes.byref(cfg))
+        cfg.block = self.B
+        cfg.validate_group = self.validate_group
+        cfg.budget_bytes = self.budget_bytes
+        for n in range(24):
+            cfg.capacity[n] = max(1, int(self.capacity(n))) if self.capacity is not None else 0
+        cfg.device = self.device
+        cfg.tune = 1 if self.tune else 0
+        cfg.keep_digits = 1 if self.keep_digits else 0
+        cfg.idle_close_s = self.idle_close_s
+        return cfg
 
-    def _pool_should_close(self, pool: _Pool, idle_since: float) -> bool:
-        if self.waiting[pool.n]:
-            return False
-        if self._dispatch_done and not any(self.waiting.values()):
-            return True
-        return (self.clock() - idle_since) > self.idle_close_s
-
-    def _close_pool(self, pool: _Pool):
-        if pool in self.pools:
-            self.pools.remove(pool)
-            self.budget.give(pool.n, pool.nbytes)
-            self.cv.notify_all()
-
-    def _place(self):
-        """Opens pools for waiting requests while the budget allows."""
-        for n, q in self.waiting.items():
-            if not q:
-                continue
-            anyb = [r for r in q if not _packed_pool(r.job.b, n)]   # need a pool that takes every base
-            packb = [r for r in q if _packed_pool(r.job.b, n)]
-            free_any = sum(p.free_slots() for p in self.pools if p.n == n and not p.packed_only)
-            free_pk = sum(p.free_slots() for p in self.pools if p.n == n and p.packed_only)
-            while True:
-                if free_any < len(anyb):
-                    rep, is_pk = 1024, False
-                elif free_pk + (free_any - len(anyb)) < len(packb):
-                    rep, is_pk = packb[0].job.b, True
-                else:
-                    break
-                cap = max(1, int(self.capacity(n)))
-                nb = cap * (slot_bytes(n) + self._exp_bytes[n])
-                if not self.budget.take(n, nb):
-                    break
-                p = _Pool(self, self._next_pid, n, cap, nb, rep_b=rep)
-                self._next_pid += 1
-                self.pools.append(p)
-                self.stats.pools_created += 1
-                p.thread.start()
-                if is_pk:
-                    free_pk += cap
-                else:
-                    free_any += cap
-
-    # -------------------------------------------------- from pool threads
-    def _finished(self, pool: _Pool, slot: int, act: _Active, x: np.ndarray, d: np.ndarray):
-        with self.cv:
-            pool.slots[slot] = None
-            job = act.req.job
-            self.completions.append(act.comp)
-            if self.validate:
-                self.vqueue[pool.n].append((act.comp, job, x, d))
-            self.cv.notify_all()
-
-    # -------------------------------------------------------- validators
-    def _validator(self, n: int):
-        """Gerbicz-Li checks of finished tests of size n, up to validate_group
-        at once, on a batch and stream of its own."""
-        bt: Optional[Batch] = None
-        q = self.vqueue[n]
-        try:
-            while True:
-                with self.cv:
-                    while not q and not self._stop_validator:
-                        self.cv.wait(0.01)
-                    if not q:
-                        break
-                    group = [q.popleft() for _ in range(min(len(q), self.validate_group))]
-                if bt is None:
-                    bt = Batch([1024] * self.validate_group, n, num_regs=NUM_REGS, device=self.device)
-                zero = np.zeros(1 << n, dtype=np.int32)
-                res = []
-                for i in range(self.validate_group):
-                    if i < len(group):
-                        c, job, x, d = group[i]
-                        bt.assign(i, c.b)
-                        bt.put(i, x, 0)
-                        bt.put(i, d, 1)
-                        res.append(chunk_sum(job.words, job.nbits, self.B))
-                    else:
-                        bt.put(i, zero, 0)
-                        bt.put(i, zero, 1)
-                        res.append(0)
-                ok = gl_validate(bt, self.B, res)
-                now = self.clock()
-                with self.cv:
-                    for i, (c, _, _, _) in enumerate(group):
-                        c.gl_ok = bool(ok[i])
-                        c.validated_at = now
-                    self.cv.notify_all()
-        except BaseException as e:
-            with self.cv:
-                self.errors.append(e)
-                self.cv.notify_all()
-        finally:
-            if bt is not None:
-                bt.close()
-
-    def _validator_bytes(self, ns: Sequence[int]) -> int:
-        return sum(self.validate_group * slot_bytes(n) for n in set(ns))
-
-    # ------------------------------------------------------------- run
     def run(self, requests: Sequence[Request], timeout_s: float = 3600.0) -> List[Completion]:
-        """Serves ``requests`` (arrival times in seconds from now) and returns
-        their completions in request order."""
+        """Serves ``requests`` (arrival times in seconds from the start of the
+        run) and returns their completions in request order."""
         reqs = sorted(requests, key=lambda r: (r.arrival, r.id))
-        ns = sorted({int(r.job.n) for r in reqs})
-        self.waiting: Dict[int, Deque[Request]] = {n: collections.deque() for n in ns}
-        self.vqueue: Dict[int, Deque] = {n: collections.deque() for n in ns}
-        self.pools: List[_Pool] = []
-        self.completions: List[Completion] = []
-        self.errors = []
-        self.stats = ServeStats(requests=len(reqs), budget_bytes=self.budget.limit)
-        # every slot of a pool may hold the longest exponent of its size
-        self._exp_bytes = {n: max(exponent_bytes(((r.job.nbits + self.B - 1) // self.B) * self.B)
-                                  for r in reqs if int(r.job.n) == n) for n in ns}
-        self._next_pid = 0
-        self._dispatch_done = False
-        self._stop_validator = False
-        vbytes = 0
-        if self.validate:
-            vbytes = self._validator_bytes(ns)
-            if vbytes > self.budget.limit:
-                raise ValueError("budget smaller than the validators' memory")
-            self.budget.limit -= vbytes
-        if self.tuner is not None:               # plans chosen before the clock starts
-            for n in ns:
-                reps = [1024] + [next((int(r.job.b) for r in reqs if int(r.job.n) == n and _packed_pool(r.job.b, n)), 1024)]
-                for rep in sorted(set(reps)):
-                    with Batch([rep] * max(1, int(self.capacity(n))), n, num_regs=NUM_REGS, device=self.device) as bt:
-                        self.tuner.tune(bt)
-        self._t0 = time.perf_counter()
-        vths = [threading.Thread(target=self._validator, args=(n,), name=f"validator-n{n}", daemon=True)
-                for n in ns] if self.validate else []
-        for v in vths:
-            v.start()
-        k = 0
-        deadline = timeout_s
+        L = self.L
+        h = vp()
+        cfg = self._config()
+        self._check(L.gfc_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        comps: Dict[int, Completion] = {}
         try:
-            with self.cv:
-                while True:
-                    now = self.clock()
-                    while k < len(reqs) and reqs[k].arrival <= now:
-                        self.waiting[int(reqs[k].job.n)].append(reqs[k])
-                        k += 1
-                    self._place()
-                    self.cv.notify_all()
-                    if self.errors:
-                        raise self.errors[0]
-                    if k == len(reqs):
-                        self._dispatch_done = True
-                        if len(self.completions) == len(reqs):
-                            break
-                    if now > deadline:
-                        raise TimeoutError("serving run exceeded its time limit")
-                    wait = 0.01 if k == len(reqs) else max(0.0, min(0.01, reqs[k].arrival - now))
-                    self.cv.wait(wait)
-                while any(p.thread.is_alive() for p in list(self.pools)):
-                    self.cv.notify_all()
-                    self.cv.wait(0.01)
-                    if self.errors:
-                        raise self.errors[0]
-                self._stop_validator = True
-                self.cv.notify_all()
+            if self.tune:                       # plans chosen before the clock starts
+                for n in sorted({int(r.job.n) for r in reqs}):
+                    reps = {1024} | {int(r.job.b) for r in reqs if int(r.job.n) == n and _packed_pool(r.job.b, n)}
+                    for rep in sorted(reps)[:2]:
+                        self._check(L.gfc_server_pretune(h, n, rep))
+            t0 = L.gfc_server_clock(h)
+            buf = (CompletionC * 64)()
+            got = ctypes.c_size_t(0)
+            k = 0
+            deadline = t0 + timeout_s
+            while len(comps) < len(reqs):
+                now = L.gfc_server_clock(h)
+                while k < len(reqs) and t0 + reqs[k].arrival <= now:
+                    j = reqs[k].job
+                    w = np.ascontiguousarray(j.words, dtype=np.uint32)
+                    self._check(L.gfc_server_submit(h, reqs[k].id, int(j.b), int(j.n),
+                                                    w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), int(j.nbits)))
+                    k += 1
+                if now > deadline:
+                    raise TimeoutError("serving run exceeded its time limit")
+                wait_ms = 5 if k == len(reqs) else int(max(0.0, min(0.005, t0 + reqs[k].arrival - now)) * 1000)
+                self._check(L.gfc_server_poll(h, buf, 64, ctypes.byref(got), wait_ms))
+                for i in range(got.value):
+                    c = buf[i]
+                    comp = Completion(int(c.id), int(c.b), int(c.n), int(c.nbits), c.arrival - t0, c.admitted - t0,
+                                      c.residue_at - t0, (c.validated_at - t0) if c.validated_at >= 0 else None,
+                                      bool(c.is_prp), int(c.res64), int(c.old64),
+                                      None if c.gl_ok < 0 else bool(c.gl_ok), int(c.pool), int(c.slot),
+                                      int(c.plan))
+                    if self.keep_digits:
+                        d = np.empty(1 << comp.n, dtype=np.int32)
+                        self._check(L.gfc_server_digits(h, comp.id, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                        d.size))
+                        comp.digits = d
+                    comps[comp.id] = comp
+            st = ServerStatsC()
+            self._check(L.gfc_server_get_stats(h, ctypes.byref(st)))
         finally:
-            self._dispatch_done = True
-            self._stop_validator = True
-            with self.cv:
-                self.cv.notify_all()
-        for v in vths:
-            v.join(timeout=max(1.0, deadline - self.clock() + 60))
-        for p in list(self.pools):
-            p.thread.join(timeout=5)
-        self.budget.limit += vbytes
-        if self.errors:
-            raise self.errors[0]
-        self._summarise()
-        order = {r.id: i for i, r in enumerate(requests)}
-        return sorted(self.completions, key=lambda c: order[c.id])
+            L.gfc_server_destroy(h)
+        self._summarise(reqs, list(comps.values()), st)
+        return [comps[r.id] for r in requests]
 
-    def _summarise(self):
-        st = self.stats
-        cs = self.completions
-        st.completed = len(cs)
+    def _summarise(self, reqs, cs: List[Completion], st: ServerStatsC):
+        s = ServeStats(requests=len(reqs), completed=len(cs), pools_created=int(st.pools_created),
+                       blocks_run=int(st.blocks_run), peak_bytes=int(st.peak_bytes), budget_bytes=int(st.budget_bytes),
+                       gl_failures=int(st.gl_failures))
+        self.stats = s
         if not cs:
             return
-        t_first = min(c.arrival for c in cs)
-        t_last = max(c.residue_at for c in cs)
-        st.seconds = t_last - t_first
-        st.digit_squarings = float(sum((1 << c.n) * c.nbits for c in cs))
+        s.seconds = max(c.residue_at for c in cs) - min(c.arrival for c in cs)
+        s.digit_squarings = float(sum((1 << c.n) * c.nbits for c in cs))
         lat = np.array([c.latency for c in cs])
-        st.p50, st.p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+        s.p50, s.p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
         vl = np.array([c.validated_at - c.arrival for c in cs if c.validated_at is not None])
         if vl.size:
-            st.p50_validated, st.p99_validated = float(np.percentile(vl, 50)), float(np.percentile(vl, 99))
-        st.mean_wait = float(np.mean([c.admitted - c.arrival for c in cs]))
-        st.peak_bytes = self.budget.peak
-        st.gl_failures = sum(1 for c in cs if c.gl_ok is False)
+            s.p50_validated, s.p99_validated = float(np.percentile(vl, 50)), float(np.percentile(vl, 99))
+        s.mean_wait = float(np.mean([c.admitted - c.arrival for c in cs]))
         for n in sorted({c.n for c in cs}):
             sub = [c for c in cs if c.n == n]
-            st.per_n[n] = {"tests": len(sub), "p50_s": float(np.median([c.latency for c in sub])),
-                           "digit_squarings": float(sum((1 << n) * c.nbits for c in sub))}
+            s.per_n[n] = {"tests": len(sub), "p50_s": float(np.median([c.latency for c in sub])),
+                          "digit_squarings": float(sum((1 << n) * c.nbits for c in sub))}
 
 
 # ------------------------------------------------------------------ the serving workload

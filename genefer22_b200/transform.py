@@ -87,6 +87,18 @@ class Batch:
         check(lib().gfc_batch_assign(self._h, test, b))
         self.bases[test] = b
 
+    def reserve(self, max_bits: int):
+        """Room for exponents of up to max_bits bits in every slot, once, so that
+        ``admit`` allocates nothing and never synchronises (gfc_batch_reserve)."""
+        check(lib().gfc_batch_reserve(self._h, int(max_bits)))
+
+    def admit(self, test: int, b: int, words: np.ndarray, nbits: int):
+        """A new test in slot ``test``: base b, r0 = r1 = 1, exponent, position;
+        enqueued on the batch stream (gfc_batch_admit)."""
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        check(lib().gfc_batch_admit(self._h, test, int(b), w.ctypes.data_as(c_u32p), int(nbits)))
+        self.bases[test] = b
+
     def set_pos(self, pos: Sequence[int]):
         p = np.ascontiguousarray(np.asarray(pos, dtype=np.int64))
         check(lib().gfc_batch_set_pos(self._h, p.ctypes.data_as(c_i64p)))

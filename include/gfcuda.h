@@ -142,6 +142,44 @@ int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *words, ui
  * gfc_graph_launch (GFC_ERR_STATE); four-step graphs stay valid. */
 int gfc_batch_assign(gfc_batch *bt, size_t test, uint32_t b);
 
+/* Reserved slots (no counterpart in the reference, which runs one test per
+ * transform; used by the serving loop, gfc_server_*).  gfc_batch_reserve
+ * allocates, once, room for an exponent of up to max_bits bits in every slot
+ * and pinned host staging; afterwards gfc_batch_admit and gfc_batch_set_exponent
+ * (for nbits <= max_bits) allocate nothing and do not synchronise: they
+ * enqueue their copies on the batch stream and return. */
+int gfc_batch_reserve(gfc_batch *bt, uint64_t max_bits);
+
+/* Admits a new test into slot `test` of a reserved batch: base b (its prime
+ * set and carry constants), r_0 = r_1 = 1 (genefer's start, src/genefer.h:492-497),
+ * exponent words (nbits <= max_bits) and bit position nbits - 1, as one
+ * asynchronous sequence on the batch stream.  `words` may be reused when the
+ * call returns.  A change of prime set under the single-CTA plan makes graphs
+ * captured before it refuse to launch (GFC_ERR_STATE), as gfc_batch_assign. */
+int gfc_batch_admit(gfc_batch *bt, size_t test, uint32_t b, const uint32_t *words, uint64_t nbits);
+
+/* Register `reg` of one test to / from host memory, enqueued on the batch
+ * stream without waiting: the host buffer (pinned for a truly asynchronous
+ * copy) must stay valid until the stream has passed the copy. */
+int gfc_batch_get_async(gfc_batch *bt, size_t test, size_t reg, int32_t *out);
+int gfc_batch_set_async(gfc_batch *bt, size_t test, size_t reg, const int32_t *in);
+
+/* Plan codes the engine accepts at size n (see gfc_batch_set_plan), in the
+ * order gfc_batch_tune measures them; *count receives their number (up to
+ * `cap` are written). */
+int gfc_plan_candidates(uint32_t n, int32_t *plans, size_t cap, size_t *count);
+
+/* Autotuner (no counterpart in the reference's OpenCL path, which picks its
+ * kernel split by its own timing loop, src/transformGPU.h:841-900): for every
+ * candidate plan the batch can take, `squarings` squarings of register 0 are
+ * captured in a CUDA graph and replayed `replays` times between CUDA events;
+ * the plan with the least device time per squaring is set (ties: the lower
+ * code) and register 0 is cleared.  plans[i], us[i] (microseconds per batch
+ * squaring) for i < min(cap, *count); *best the chosen plan.  Squares register 0
+ * in place: tune a batch before loading its tests. */
+int gfc_batch_tune(gfc_batch *bt, uint32_t squarings, uint32_t replays, int32_t *plans, float *us, size_t cap,
+				   size_t *count, int32_t *best);
+
 /* Sets every test's bit position (pos[i] < 0: the test has finished). */
 int gfc_batch_set_pos(gfc_batch *bt, const int64_t *pos);
 int gfc_batch_get_pos(gfc_batch *bt, int64_t *pos);
@@ -249,6 +287,94 @@ int gfc_probe_int_throughput(int device, double *out);
  *    GFC_ERR_NUMERIC. */
 int gfc_square_noalloc(const int32_t *in, int32_t *out, uint32_t b, uint32_t n, int dup, uint32_t count, int device,
 					   void *stream);
+
+/* ------------------------------------------------------------------ serving
+ * No counterpart in the reference, which runs one test per process
+ * (src/genefer.h:1360-1480).  A continuous-batching request loop on one
+ * device, run by a native dispatcher thread: tests of one size n share a pool
+ * of slots (one batch, its block of genefer's prp loop as one CUDA graph:
+ * the Gerbicz-Li update d <- d x, src/genefer.h:529-535, then `block`
+ * squarings with each slot's own exponent bits).  Between two blocks of a
+ * pool, finished tests are read back and waiting tests of that size are
+ * admitted into free slots (gfc_batch_admit: no allocation, no
+ * synchronisation), so the pools' blocks keep overlapping on the device.
+ * Pools open while the device-memory budget allows and close when idle.
+ * Finished tests get genefer's Gerbicz-Li check (src/genefer.h:557-615),
+ * validate_group of one size at once, on a checker batch of their own.
+ * Every test reads only its own slot, base and exponent bits, so its residue
+ * is the same alone and among others. */
+typedef struct gfc_server gfc_server;
+
+typedef struct gfc_server_config
+{
+	uint32_t block;           /* Gerbicz-Li block length B (squarings per block) */
+	uint32_t validate_group;  /* finished tests checked together (0: no check) */
+	uint64_t budget_bytes;    /* device memory pools and checkers may hold */
+	uint32_t capacity[24];    /* slots per pool, by n (0: the default for n) */
+	int32_t device;           /* CUDA ordinal */
+	int32_t tune;             /* 1: autotune each pool shape's plan (cached per shape) */
+	int32_t keep_digits;      /* 1: keep canonical residues for gfc_server_digits */
+	double idle_close_s;      /* a pool with no test and nothing waiting closes after this */
+} gfc_server_config;
+
+typedef struct gfc_completion
+{
+	uint64_t id, nbits;
+	uint32_t b, n;
+	double arrival, admitted, residue_at, validated_at;  /* seconds on gfc_server_clock; validated_at < 0: unchecked */
+	uint64_t res64, old64;    /* gint::isOne (src/gint.h:169-202) of the residue */
+	int32_t is_prp, gl_ok;    /* gl_ok: 1 passed, 0 failed, -1 not checked */
+	int32_t pool, slot, plan; /* the pool, its slot and the pool's kernel plan (gfc_batch_set_plan) */
+} gfc_completion;
+
+typedef struct gfc_server_stats
+{
+	uint64_t submitted, completed, pools_created, pools_open, blocks_run;
+	uint64_t used_bytes, peak_bytes, budget_bytes, gl_failures;
+} gfc_server_stats;
+
+/* block 1000, validate_group 4, budget 80 GB, default capacities, device 0,
+ * tuning on, digits not kept, idle_close_s 0.25. */
+void gfc_server_default_config(gfc_server_config *cfg);
+
+/* Starts the loop's threads; the server clock starts now. */
+int gfc_server_create(const gfc_server_config *cfg, gfc_server **out);
+
+/* Tunes the plan of the pools of size n (bases like rep_b) before requests
+ * arrive, so that opening a pool later does not measure plans. */
+int gfc_server_pretune(gfc_server *s, uint32_t n, uint32_t rep_b);
+
+/* Queues a request: base b, size n (8 <= n <= 23), the exponent's nbits bits
+ * (a whole test, b^(2^n), or its top bits: the state after that many
+ * squarings of genefer's prp loop).  Its arrival time is now. */
+int gfc_server_submit(gfc_server *s, uint64_t id, uint32_t b, uint32_t n, const uint32_t *words, uint64_t nbits);
+
+/* Completed requests (checked, when checking is on), up to cap; waits up to
+ * wait_ms for the first.  A failure of the loop is returned here. */
+int gfc_server_poll(gfc_server *s, gfc_completion *out, size_t cap, size_t *got, int32_t wait_ms);
+
+/* Canonical residue digits of a completed request (keep_digits), once. */
+int gfc_server_digits(gfc_server *s, uint64_t id, int32_t *out, size_t size);
+
+int gfc_server_get_stats(gfc_server *s, gfc_server_stats *out);
+double gfc_server_clock(const gfc_server *s);
+
+/* Stops the loop after the device work in flight; releases everything. */
+void gfc_server_destroy(gfc_server *s);
+
+/* Device bytes the server's budget counts: one pool slot of size n holding an
+ * exponent of up to max_bits bits, and the root tables of size n (counted
+ * once per size while a pool or checker of that size is open); the default
+ * slots per pool. */
+uint64_t gfc_server_slot_bytes(uint32_t n, uint64_t max_bits);
+uint64_t gfc_server_table_bytes(uint32_t n);
+uint32_t gfc_server_default_capacity(uint32_t n);
+
+/* Range checks on the host: the RNS width (2 or 3) the engine picks for
+ * (b, n) with one digit per coefficient, or GFC_ERR_ARG / GFC_ERR_RANGE;
+ * whether b is in the packed-digit range at n (1 or 0). */
+int gfc_width_for(uint32_t b, uint32_t n);
+int gfc_packed_range(uint32_t b, uint32_t n);
 
 /* ------------------------------------------------------------------ residues (host)
  * genefer's gint utilities on N host digits (src/gint.h:40-225). */

@@ -186,3 +186,42 @@ def test_serve_with_large_test():
     r = next(r for r in reqs if r.job.n == 23)
     _, alone = run_alone(r.job, B)
     assert np.array_equal(alone, big[0].digits)
+
+
+def test_admission_leaves_other_pools_running(oracle):
+    """Admitting a test into one pool (gfc_batch_admit) neither allocates device
+    memory nor waits for another pool's graph in flight: right after the call
+    returns, the other pool's replay is still running; the admitted test then
+    squares like a fresh test."""
+    import torch
+    B = 8
+    big = Batch([30_000_002] * 2, 20)
+    g = big.capture(lambda: big.square(False, 400))        # about 20 ms of device work
+    small = Batch([1_000_002, 1_999_999_998], 12)
+    small.reserve(4 * B)
+    job = gf.Job.prefix(2_000_000_000 - 2, 12, 3 * B)
+    s_big = torch.cuda.ExternalStream(big.stream)
+    ev = torch.cuda.Event()
+    g.launch()
+    ev.record(s_big)
+    free0 = torch.cuda.mem_get_info(0)[0]
+    small.admit(1, job.b, job.words, job.nbits)            # prime set changes too (2 -> 3 primes)
+    assert not ev.query(), "admission waited for the other pool's graph"
+    assert torch.cuda.mem_get_info(0)[0] >= free0
+    small.square_exp(job.nbits)
+    assert np.array_equal(canon(small.get(1, 0), job.b), oracle_prefix(oracle, job, 10**9))
+    g.close()
+
+
+def test_native_server_reports_plans_and_stats():
+    """The native loop's completions carry the pool's plan and the stats its
+    counters: blocks run, pools opened, peak memory within the budget."""
+    B = 16
+    reqs = serve_requests(count=6, rate=100.0, blocks=[2], B=B, seed=3, ns=(15, 16), big=None)
+    srv = Server(B=B, budget_bytes=4 * 10**9, validate_group=2, keep_digits=False)
+    comps = srv.run(reqs, timeout_s=300)
+    assert all(c.gl_ok for c in comps)
+    assert all(c.plan in candidates(c.n) for c in comps)
+    st = srv.stats
+    assert st.blocks_run >= 2 and 1 <= st.pools_created and st.peak_bytes <= 4 * 10**9
+    assert st.p50 <= st.p99

