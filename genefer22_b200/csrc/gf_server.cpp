@@ -282,8 +282,6 @@ void Server::step(bool &progress)
 		std::lock_guard<std::mutex> l(in_mu_);
 		for (Req &r : incoming_)
 		{
-			const uint64_t pad = ((r.nbits + cfg_.block - 1) / cfg_.block) * cfg_.block;
-			max_bits_[r.n] = std::max(max_bits_[r.n], pad);
 			waiting_[r.n].push_back(std::move(r));
 			progress = true;
 		}
@@ -444,7 +442,9 @@ void Server::place()
 			else if (free_pk + (free_any - any_w) < pk_w) { rep = pk_rep; pk = true; }
 			else break;
 			const uint32_t cap = (cfg_.capacity[n] != 0) ? cfg_.capacity[n] : default_capacity(n);
-			const uint64_t mb = max_bits_[n];
+			// every slot can hold the longest exponent of its size: b < 2^31 gives
+			// b^(2^n) fewer than 31 2^n bits, padded to whole blocks
+			const uint64_t mb = (uint64_t(31) << n) + cfg_.block;
 			const uint64_t bytes = cap * (slot_bytes(n) + exponent_bytes(mb));
 			// the first pool of a size also brings the size's checker
 			const bool need_check = (cfg_.validate_group > 0) && (checkers_.count(n) == 0 || checkers_[n].bytes == 0);

@@ -205,7 +205,6 @@ private:
 	std::map<uint32_t, std::deque<Req>> waiting_;
 	std::vector<std::unique_ptr<Pool>> pools_;
 	std::map<uint32_t, Checker> checkers_;
-	std::map<uint32_t, uint64_t> max_bits_;     // longest padded exponent seen per size
 	int next_pid_ = 0;
 	uint64_t used_ = 0, peak_ = 0;
 	std::map<uint32_t, int> tables_;            // pools + checkers holding each size's tables

@@ -67,6 +67,13 @@ def slot_bytes(n: int, max_bits: int = 0) -> int:
     return int(_default_lib().gfc_server_slot_bytes(int(n), int(max_bits)))
 
 
+def pool_slot_bytes(n: int, B: int) -> int:
+    """Device bytes of one slot of a serving pool of size n and block length B:
+    the slot holds room for the longest exponent of its size (b < 2^31, so
+    b^(2^n) has fewer than 31 2^n bits), padded to whole blocks."""
+    return slot_bytes(n, (31 << int(n)) + int(B))
+
+
 def table_bytes(n: int) -> int:
     """Root tables of size n, counted once per size while a pool of it is open."""
     return int(_default_lib().gfc_server_table_bytes(int(n)))

@@ -68,7 +68,7 @@ bool bit(const std::vector<uint32_t> &w, uint64_t i) { return ((w[i >> 5] >> (i 
 class FakePool : public gfs::PoolDev
 {
 public:
-	FakePool(uint32_t n, size_t cap, uint32_t B) : n_(n), B_(B), slots_(cap) {}
+	FakePool(uint32_t n, size_t cap, uint32_t B, uint64_t max_bits) : n_(n), B_(B), max_bits_(max_bits), slots_(cap) {}
 	~FakePool() override
 	{
 		for (int32_t *p : bufs_) std::free(p);
@@ -76,6 +76,8 @@ public:
 	int plan() const override { return 0; }
 	void admit(size_t slot, uint32_t b, const uint32_t *words, uint64_t nbits) override
 	{
+		// the engine's reserved exponent room (gfc_batch_admit refuses longer exponents)
+		if ((nbits == 0) || (nbits > max_bits_)) throw gfs::Error{ GFC_ERR_ARG, "admit: need 1 <= nbits <= the reserved bits" };
 		Slot &s = slots_[slot];
 		s.o.reset(new Oracle(b, n_));
 		gfo_set(s.o->h, 1);
@@ -130,6 +132,7 @@ private:
 		uint32_t blocks = 0;
 	};
 	uint32_t n_, B_;
+	uint64_t max_bits_;
 	std::vector<Slot> slots_;
 	std::vector<int32_t *> bufs_;
 };
@@ -174,9 +177,9 @@ private:
 class FakeDevices : public gfs::Devices
 {
 public:
-	gfs::PoolDev *open_pool(uint32_t n, size_t capacity, uint32_t, uint32_t B, uint64_t, bool) override
+	gfs::PoolDev *open_pool(uint32_t n, size_t capacity, uint32_t, uint32_t B, uint64_t max_bits, bool) override
 	{
-		return new FakePool(n, capacity, B);
+		return new FakePool(n, capacity, B, max_bits);
 	}
 	gfs::CheckDev *open_check(uint32_t n, size_t, uint32_t B) override { return new FakeCheck(n, B); }
 	bool valid(uint32_t b, uint32_t) override { return (b >= 8) && (b < (1u << 31)); }

@@ -11,7 +11,7 @@ from genefer22_b200 import genefer as gf
 from genefer22_b200.autotune import Autotuner, candidates
 from genefer22_b200.exponent import words_to_int
 from genefer22_b200.mixed import MixedBatch, run_alone, uneven_tests
-from genefer22_b200.serve import Server, serve_requests, slot_bytes, table_bytes
+from genefer22_b200.serve import Server, pool_slot_bytes, serve_requests, slot_bytes, table_bytes
 
 pytestmark = pytest.mark.gpu
 
@@ -156,8 +156,8 @@ def test_serve_alone_vs_mix(oracle):
     B = 32
     reqs = serve_requests(count=14, rate=200.0, blocks=[2, 3], B=B, seed=1005, ns=(15, 16, 17), big=None)
     ns = (15, 16, 17)
-    budget = (sum(2 * slot_bytes(n) + table_bytes(n) for n in ns)     # validators, root tables
-              + 2 * 2 * (slot_bytes(17) + 4096))                        # two pools of two slots
+    budget = (sum(2 * slot_bytes(n, B + 64) + table_bytes(n) for n in ns)   # checkers, root tables
+              + 2 * 2 * pool_slot_bytes(17, B))                               # two pools of two slots
     srv = Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True)
     comps = srv.run(reqs, timeout_s=600)
     st = srv.stats

@@ -102,6 +102,7 @@ def test_budget_sizes():
         N = 1 << n
         assert sv.slot_bytes(n) >= 3 * 4 * N + 24 * N + (N // 16) * 40
         assert sv.slot_bytes(n, 4096) - sv.slot_bytes(n) == 512
+        assert sv.pool_slot_bytes(n, 1000) == sv.slot_bytes(n, 31 * N + 1000)
         assert sv.table_bytes(n) == 96 * N
     assert [sv.default_capacity(n) for n in (15, 17, 20, 22)] == [32, 16, 2, 1]
 
@@ -165,8 +166,7 @@ def _requests(B, count=10, seed=5):
 
 def _budget(ns, cap, group, B):
     """Pools of `cap` slots for every size at once, their checkers and tables."""
-    mb = 3 * B
-    return sum(cap * sv.slot_bytes(n, mb) + group * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
+    return sum(cap * sv.pool_slot_bytes(n, B) + group * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
 
 
 def test_serve_loop_on_oracle(fake_lib, oracle):
@@ -195,8 +195,7 @@ def test_serve_budget_rotates_pools(fake_lib, oracle):
     reqs = _requests(B, count=8, seed=11)
     ns = sorted({r.job.n for r in reqs})
     assert len(ns) >= 2
-    mb = 3 * B
-    one = max(2 * sv.slot_bytes(n, mb) + sv.table_bytes(n) for n in ns)
+    one = max(2 * sv.pool_slot_bytes(n, B) + sv.table_bytes(n) for n in ns)
     checkers = sum(2 * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
     budget = one + checkers
     srv = sv.Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True,
@@ -278,3 +277,19 @@ def test_uneven_batch_through_native_loop(fake_lib, oracle, monkeypatch):
     for j, c in zip(jobs, mb.residues()):
         assert np.array_equal(c, _oracle_prefix(oracle, j, B))
     assert mb.stats.digit_squarings == sum((1 << j.n) * j.nbits for j in jobs)
+
+
+def test_serve_longer_exponent_after_pool_opened(fake_lib, oracle):
+    """A pool reserves room for the longest exponent of its size, so a request
+    whose exponent is far longer than those the pool opened for is admitted
+    into it later."""
+    B = 6
+    short = gf.Job.prefix(1_000_002, 9, 2 * B)
+    long = gf.Job.prefix(1_000_004, 9, 40 * B)
+    reqs = [sv.Request(0, short, 0.0), sv.Request(1, long, 0.05)]
+    srv = sv.Server(B=B, budget_bytes=10**9, capacity=lambda n: 1, validate_group=1, keep_digits=True,
+                    idle_close_s=10.0, lib=fake_lib)
+    comps = srv.run(reqs, timeout_s=120)
+    assert srv.stats.pools_created == 1
+    for r, c in zip(reqs, comps):
+        assert c.gl_ok and np.array_equal(c.digits, _oracle_prefix(oracle, r.job, B))
