@@ -411,12 +411,10 @@ def run_uneven(args):
     from genefer22_b200.mixed import MixedBatch, uneven_tests
     torch.cuda.set_device(0)
     tests = uneven_tests(256, seed=1004)
-    warm = MixedBatch([Job.prefix(b, n, BLOCK) for b, n in tests], B=BLOCK, tuner=Autotuner())
-    warm.run(validate=False)
     jobs = [Job.prefix(b, n, args.steps * BLOCK) for b, n in tests]
     mb = MixedBatch(jobs, B=BLOCK, tuner=Autotuner())
     with Clocks(0) as ck:
-        res = mb.run(validate=True)
+        res = mb.run(validate=True, warmup=True)       # a first wave opens the pools
     st = mb.stats
     per_class = {}
     plain_s = 0.0
@@ -432,7 +430,9 @@ def run_uneven(args):
             "config": {"workload": "uneven batch of 256 tests, n 12..18 (40/20/15/10/8/5/2 %), b log-uniform "
                                    "[1024,2e9) clipped per n, seed 1004, Gerbicz-Li block of 1000 squarings, "
                                    "native loop (one pool per size class)",
-                       "classes": per_class, "timing": "host clock, submission to the last residue read back"},
+                       "classes": per_class,
+                       "timing": "host clock, submission of the second wave (pools opened by a first wave of one "
+                                 "block per test) to the last residue read back"},
             "gl_failures": sum(1 for r in res if not r.gl_ok),
             "plain": {"value": plain, "what": "each test alone, one gfc_square_dup call per squaring"},
             "mixed_over_plain": st.rate / plain, "clocks": ck.summary()}
@@ -469,6 +469,8 @@ def run_serve(args):
             "p50_time_to_validated_s": st.p50_validated, "p99_time_to_validated_s": st.p99_validated,
             "mean_queue_wait_s": st.mean_wait, "completed": st.completed, "gl_failures": st.gl_failures,
             "pools_created": st.pools_created, "blocks_run": st.blocks_run, "peak_budget_bytes": st.peak_bytes,
+            "open_s_sum": st.open_s_sum, "open_s_max": st.open_s_max, "dispatcher_step_s_max": st.step_s_max,
+            "saturated_open_s": {"sum": cap.open_s_sum, "max": cap.open_s_max, "step_max": cap.step_s_max},
             "saturated": {"value": cap.rate, "seconds": cap.seconds, "p50_s": cap.p50, "p99_s": cap.p99},
             "per_n": {str(k): v for k, v in st.per_n.items()},
             "clocks": ck.summary()}

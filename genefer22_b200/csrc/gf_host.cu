@@ -128,29 +128,38 @@ inline void put_root(uint32_t *t, size_t k, uint32_t w, uint32_t p)
 }
 
 // Root tables of one prime for length N = 2^n (N entries of root_words(p)
-// words; layout in gf_ntt.cuh):
+// words; layout in gf_ntt.cuh), built on the device (k_roots):
 //   entry k of fw = psi^bitrev_n(k), of iv = psi^-bitrev_n(k)  (k >= 1),
-//   word 0 of fw = R^2 / N (normalisation c), of iv = psi^(-N/2) c (K), in
-//   Montgomery form (R = 2^32).  `pw` is scratch for N + 1 powers.
-void build_roots(uint32_t p, int n, uint32_t *fw, uint32_t *iv, uint32_t *pw)
+//   word 0 of fw = R^2 / N (normalisation c), of iv = psi^(-N/2) c (k0), in
+//   Montgomery form (R = 2^32).
+// The host finds psi and the entry-0 constants; the kernel writes the N
+// entries of both tables with one product per entry.  fw and iv are device
+// pointers; `s` a stream of the device.
+void build_roots_device(uint32_t p, int n, uint32_t *fw, uint32_t *iv, cudaStream_t s)
 {
 	const uint32_t N = 1u << n;
 	const uint32_t psi = powmod_h(primitive_root(p), (p - 1) / (2ull * N), p);
-	pw[0] = 1;
-	for (uint32_t i = 1; i <= N; ++i) pw[i] = mulmod_h(pw[i - 1], psi, p);
-	if (pw[N] != p - 1) fail(GFC_ERR_ARG, "root table: psi is not a primitive 2N-th root");
-	for (uint32_t k = 1; k < N; ++k)
-	{
-		const uint32_t e = bitrev(k, n);
-		put_root(fw, k, pw[e], p);
-		put_root(iv, k, p - pw[N - e], p);
-	}
+	if (powmod_h(psi, N, p) != p - 1) fail(GFC_ERR_ARG, "root table: psi is not a primitive 2N-th root");
+	const uint32_t psi_inv = powmod_h(psi, 2ull * N - 1, p);
 	const uint32_t R1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
 	const uint32_t c = mulmod_h(mulmod_h(R1, R1, p), powmod_h(N % p, p - 2, p), p);
-	fw[0] = c;
-	iv[0] = mulmod_h(p - pw[N / 2], c, p);
-	if (root_words(p) == 2) { fw[1] = 0; iv[1] = 0; }
+	const uint32_t k0 = mulmod_h(p - powmod_h(psi, N / 2, p), c, p);
+	const int run = 64, threads = 256;
+	const uint32_t runs = (N + run - 1) / run;
+	k_roots<<<(runs + threads - 1) / threads, threads, 0, s>>>(fw, iv, p, psi, psi_inv, n, static_cast<int>(root_words(p)),
+															   run, c, k0);
+	const cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) fail(GFC_ERR_CUDA, std::string("root table kernel: ") + cudaGetErrorString(e));
 }
+
+// A private stream for building tables, synchronised and destroyed on scope exit.
+struct TableStream
+{
+	cudaStream_t s = nullptr;
+	TableStream() { GFC_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+	~TableStream() { if (s != nullptr) cudaStreamDestroy(s); }
+	void sync() { GFC_CK(cudaStreamSynchronize(s)); }
+};
 
 struct DeviceTables
 {
@@ -181,13 +190,14 @@ std::shared_ptr<DeviceTables> get_tables(int device, int n)
 	size_t off[5], total = 0;
 	for (int s = 0; s < 5; ++s) { off[s] = total; total += 2 * root_words(kPrime[s]) * N; }
 	GFC_CK(cudaMalloc(&t->d, total * sizeof(uint32_t)));
-	std::vector<uint32_t> fw(2 * N), iv(2 * N), pw(N + 1);
-	for (int s = 0; s < 5; ++s)
 	{
-		const size_t words = root_words(kPrime[s]) * N;
-		build_roots(kPrime[s], n, fw.data(), iv.data(), pw.data());
-		GFC_CK(cudaMemcpy(t->d + off[s], fw.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
-		GFC_CK(cudaMemcpy(t->d + off[s] + words, iv.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		TableStream ts;
+		for (int s = 0; s < 5; ++s)
+		{
+			const size_t words = root_words(kPrime[s]) * N;
+			build_roots_device(kPrime[s], n, t->d + off[s], t->d + off[s] + words, ts.s);
+		}
+		ts.sync();
 	}
 	const int slot0[2] = { 0, 2 };
 	for (int set = 0; set < 2; ++set)
@@ -229,14 +239,15 @@ std::shared_ptr<DeviceTables> get_tables_packed(int device, int np)
 	const size_t N = size_t(1) << np;
 	const size_t words = 2 * N;                       // 31-bit primes: root and Shoup quotient
 	GFC_CK(cudaMalloc(&t->d, 8 * words * sizeof(uint32_t)));
-	std::vector<uint32_t> fw(words), iv(words), pw(N + 1);
-	for (int pl = 0; pl < 4; ++pl)
 	{
-		build_roots(PrimeSet<2>::p[pl], np, fw.data(), iv.data(), pw.data());
-		GFC_CK(cudaMemcpy(t->d + (2 * pl) * words, fw.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
-		GFC_CK(cudaMemcpy(t->d + (2 * pl + 1) * words, iv.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
-		t->tab[2].fw[pl] = t->d + (2 * pl) * words;
-		t->tab[2].iv[pl] = t->d + (2 * pl + 1) * words;
+		TableStream ts;
+		for (int pl = 0; pl < 4; ++pl)
+		{
+			t->tab[2].fw[pl] = t->d + (2 * pl) * words;
+			t->tab[2].iv[pl] = t->d + (2 * pl + 1) * words;
+			build_roots_device(PrimeSet<2>::p[pl], np, t->d + (2 * pl) * words, t->d + (2 * pl + 1) * words, ts.s);
+		}
+		ts.sync();
 	}
 	g_tab_cache[key] = t;
 	return t;
@@ -474,11 +485,11 @@ void launch_pcol(int lr, bool inv, const Args &a, int grid_y, cudaStream_t s, bo
 // allows 16-CTA clusters and returns in *max_out how many clusters fit on the
 // device at once; otherwise launches a persistent grid of
 // min(ntests, max_active) clusters over the tests a.tests[0 .. ntests-1].
-template <int LQ>
+template <int LQ, int LC>
 void cluster_t(const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
 {
-	using S = ClusterShape<LQ>;
-	auto kern = k_cluster<LQ>;
+	using S = ClusterShape<LQ, LC>;
+	auto kern = k_cluster<LQ, LC>;
 	cudaLaunchConfig_t cfg = {};
 	cudaLaunchAttribute at[1];
 	at[0].id = cudaLaunchAttributeClusterDimension;
@@ -500,18 +511,32 @@ void cluster_t(const Args &a, int ntests, int max_active, cudaStream_t s, bool p
 	const int ncl = (ntests < max_active) ? ntests : max_active;
 	cfg.gridDim = dim3(static_cast<unsigned>(ncl * S::Q));
 	cfg.stream = s;
+	// programmatic stream serialization as launch_pdl: the clusters start when
+	// the previous kernel of the stream has completed (pdl_wait), its launch overlapping that kernel's tail
+	cudaLaunchAttribute at2[2] = { at[0], {} };
+	at2[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at2[1].val.programmaticStreamSerializationAllowed = 1;
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+	GFC_CK(cudaStreamIsCapturing(s, &cs));
+	cfg.attrs = at2;
+	cfg.numAttrs = (cs == cudaStreamCaptureStatusNone) ? 2 : 1;
 	GFC_CK(cudaLaunchKernelEx(&cfg, kern, a, ntests));
 	after_launch();
 }
 
-void launch_cluster_lq(int lq, const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
+// Cluster shape by size: n = 12..14 on eight CTAs with rows of 2^(n-3)
+// (plane-split passes), n = 15..17 on 2..8 CTAs with rows of 2^13.
+void launch_cluster_n(int n, const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
 {
-	switch (lq)
+	switch (n)
 	{
-		case 2: cluster_t<2>(a, ntests, max_active, s, prep, max_out); break;
-		case 3: cluster_t<3>(a, ntests, max_active, s, prep, max_out); break;
-		case 4: cluster_t<4>(a, ntests, max_active, s, prep, max_out); break;
-		default: fail(GFC_ERR_ARG, "cluster plan needs 15 <= n <= 17");
+		case 12: cluster_t<3, 9>(a, ntests, max_active, s, prep, max_out); break;
+		case 13: cluster_t<3, 10>(a, ntests, max_active, s, prep, max_out); break;
+		case 14: cluster_t<3, 11>(a, ntests, max_active, s, prep, max_out); break;
+		case 15: cluster_t<2, 13>(a, ntests, max_active, s, prep, max_out); break;
+		case 16: cluster_t<3, 13>(a, ntests, max_active, s, prep, max_out); break;
+		case 17: cluster_t<4, 13>(a, ntests, max_active, s, prep, max_out); break;
+		default: fail(GFC_ERR_ARG, "cluster plan needs 12 <= n <= 17");
 	}
 }
 
@@ -552,7 +577,17 @@ void launch_mid(int lr2, bool inv, const Args &a, int grid_y, cudaStream_t s, bo
 		case 3: midr_t<3>(inv, a, grid_y, s, prep, planes); break;
 		case 4: midr_t<4>(inv, a, grid_y, s, prep, planes); break;
 		case 5: midr_t<5>(inv, a, grid_y, s, prep, planes); break;
-		case 6: midr_t<6>(inv, a, grid_y, s, prep, planes); break;
+		case 6:
+		{
+			// 64-point columns on thread pairs (k_midp): 128 registers, four CTAs per SM
+			if (prep) break;
+			const size_t C = size_t(1) << (a.n - MID_LR1 - 6);
+			const dim3 grid(static_cast<unsigned>((size_t(1) << MID_LR1) * size_t(planes) * (C / MIDP_COLS)),
+							static_cast<unsigned>(grid_y));
+			if (inv) launch_pdl(k_midp<true>, grid, dim3(MIDP_THREADS), 0, s, a);
+			else launch_pdl(k_midp<false>, grid, dim3(MIDP_THREADS), 0, s, a);
+			break;
+		}
 		case 7: mid_t<7>(inv, a, grid_y, s, prep, planes); break;
 		default: fail(GFC_ERR_ARG, "six-step plan needs 3 <= lr2 <= 7");
 	}
@@ -563,6 +598,11 @@ constexpr int PLAN_PACKED = 200;  // plan codes 200 + lr: packed digits, four-st
 constexpr int PLAN_PACKED_SIX = 300;   // plan codes 300 + lr2: packed digits, six-step of n - 1
 
 constexpr int PLAN_CLUSTER = 1;   // plan code of the cluster-resident squaring
+// A batch of at most this many tests of size 12..14 squares on the cluster
+// plan by default: one test on eight SMs instead of one (a lone n = 12, 13,
+// 14 test 15.4 -> 12.0, 31.3 -> 11.9, 62.4 -> 14.9 us per squaring, graph
+// replay on one B200); larger batches fill the SMs with one CTA per test.
+constexpr size_t CLUSTER_MAX_TESTS = 4;
 
 bool plan_valid(int n, int lr)
 {
@@ -576,7 +616,7 @@ bool plan_valid(int n, int lr)
 		const int l = lr - PLAN_PACKED, lc = n - 1 - l;
 		return (l >= 3) && (l <= 4) && (lc >= 8) && (lc <= 13);
 	}
-	if (lr == PLAN_CLUSTER) return (n >= 13 + 2) && (n <= 13 + 4);
+	if (lr == PLAN_CLUSTER) return (n >= 12) && (n <= 17);
 	if (lr > PLAN_SIX)
 	{
 		const int lr2 = lr - PLAN_SIX, lc = n - MID_LR1 - lr2;
@@ -647,7 +687,7 @@ struct gfc_batch
 	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };   // tests per prime set; d_tests lists set 0 first
 	int pending = -1;             // register whose segment carries are not yet absorbed (four-step)
 	uint64_t sets_version = 0;    // bumped when a test changes prime set (per-set launches change)
-	int cluster = 0;              // log2 CTAs per cluster when squarings use k_cluster, else 0
+	int cluster = 0;              // 1 when squarings use k_cluster (shape by n), else 0
 	int six = 0;                  // lr2 of a six-step plan (columns 2^4 x 2^lr2, lr = 4 + lr2), else 0
 	bool packed = false;          // prime set 2, two digits per coefficient, transform of N/2 (lr of that)
 	std::shared_ptr<DeviceTables> tabp;   // root tables of prime set 2 at length N/2
@@ -740,7 +780,7 @@ void apply_plan(gfc_batch &bt, int code)
 	{
 		// products keep the default plan of 15 <= n <= 17
 		apply_plan(bt, default_plan(bt.n));
-		bt.cluster = bt.n - ClusterShape<2>::LC;
+		bt.cluster = 1;
 	}
 	else if (code > PLAN_SIX)
 	{
@@ -797,7 +837,7 @@ void launch_small(const gfc_batch &bt, const Args &a0, cudaStream_t s, bool prep
 // Cluster-resident squarings: one persistent launch over all tests.
 void launch_cluster(gfc_batch &bt, const Args &a, cudaStream_t s)
 {
-	launch_cluster_lq(bt.cluster, a, static_cast<int>(bt.count), bt.cluster_max, s, false, nullptr);
+	launch_cluster_n(bt.n, a, static_cast<int>(bt.count), bt.cluster_max, s, false, nullptr);
 }
 
 // Raises shared-memory limits of the kernels the current plan uses.
@@ -805,7 +845,7 @@ void prepare_plan(gfc_batch &bt)
 {
 	Args a{};
 	a.n = bt.n;
-	if (bt.cluster > 0) launch_cluster_lq(bt.cluster, a, 0, 0, nullptr, true, &bt.cluster_max);
+	if (bt.cluster > 0) launch_cluster_n(bt.n, a, 0, 0, nullptr, true, &bt.cluster_max);
 	if (bt.packed)
 	{
 		launch_pcol(bt.six ? MID_LR1 : bt.lr, true, a, 0, nullptr, true);
@@ -1168,6 +1208,8 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 		set_packed(*bt, true);
 		apply_plan(*bt, default_packed_plan(bt->n));
 	}
+	else if ((bt->n >= 12) && (bt->n <= SMALL_MAX_LOGN) && (count <= CLUSTER_MAX_TESTS))
+		apply_plan(*bt, PLAN_CLUSTER);
 	prepare_plan(*bt);
 	return bt.release();
 }
@@ -1987,7 +2029,7 @@ uint32_t na_primitive_root(uint32_t p)
 	}
 }
 
-// The root tables of build_roots(), written into the host staging arrays.
+// The root tables of build_roots_device(), built on the host into the staging arrays.
 void na_build_roots(uint32_t p, int n)
 {
 	const uint32_t N = 1u << n;

@@ -502,28 +502,40 @@ __global__ void __launch_bounds__(SmallShape<SET, LOGN, SPLIT>::T, SmallShape<SE
 
 // One test per thread-block cluster of Q = 2^LQ CTAs, resident in shared
 // memory for many squarings.  The test is the four-step matrix of Q rows of
-// C = 2^13 digits; CTA q holds row q (digits q C .. q C + C - 1).  Per
+// C = 2^LC digits; CTA q holds row q (digits q C .. q C + C - 1).  Per
 // squaring: the Q-point column transforms (stages 0 .. LQ-1, base 1) read and
 // write the Q rows through distributed shared memory, each CTA transforms its
 // row (stages LQ .. n-1 with base 2^LQ + q, pointwise square, inverse), the
-// inverse column transforms fold in the normalisation, and every thread turns
-// 16 consecutive digits of its row into balanced base-b digits (CRT + carry);
-// the carry out of each 16-digit segment enters the next one (across CTAs,
-// and negated from the last segment to the first: b^N = -1) before the next
-// squaring.  Digits stay in registers between squarings; global memory is
-// read when a test starts and written when it ends.  A persistent grid of
+// inverse column transforms fold in the normalisation, and every owner thread
+// turns 16 consecutive digits of its row into balanced base-b digits (CRT +
+// carry); the carry out of each 16-digit segment enters the next one (across
+// CTAs, and negated from the last segment to the first: b^N = -1) before the
+// next squaring.  Digits stay in registers between squarings; global memory
+// is read when a test starts and written when it ends.  A persistent grid of
 // clusters takes tests t = cluster, cluster + clusters, ...
-template <int LQ>
+//
+// Rows of 2^13 (n = 15..17, LQ = 2..4) have one owner thread per segment and
+// no more threads.  Shorter rows (n = 12..14 on eight CTAs, LC = 9..11) add
+// plane-split threads: the transform passes and column transforms run a thread
+// per (plane, group), three times the owners, so that a lone small test spread
+// over eight SMs still keeps several warps on each.
+template <int LQ, int LC = 13>
 struct ClusterShape
 {
 	static constexpr int Q = 1 << LQ;
-	static constexpr int LC = 13;
 	static constexpr int C = 1 << LC;
 	static constexpr int PC = C + C / 32;                 // padded plane (RowMap)
-	static constexpr int T = 512;
-	static constexpr int D = C / T;                       // digits per thread
-	static constexpr size_t SMEM = size_t(WMAX) * PC * 4 + size_t(T) * 8;
-	static_assert(D == SEG, "one carry segment per thread");
+	static constexpr bool PS = (LC <= 11);                // plane-split passes
+	// digits per owner thread: 16 (one carry segment of the engine), or 8 for
+	// the short rows, whose owners then run half as long a carry chain (the
+	// carries inside the kernel are its own; every carry fits 8 digits for
+	// b >= 1024, absorb() checks it)
+	static constexpr int D = PS ? SEG / 2 : SEG;
+	static constexpr int T0 = C / D;                      // owner threads
+	static constexpr int T = PS ? ((WMAX * C / SEG > T0) ? WMAX * C / SEG : T0) : T0;
+	static constexpr int MINB = PS ? 1 : 2;
+	static constexpr size_t SMEM = size_t(WMAX) * PC * 4 + size_t(T0) * 8;
+	static_assert(T <= 1024, "threads per CTA");
 };
 
 // Distributed shared memory by 32-bit shared::cluster addresses: the word at
@@ -545,45 +557,69 @@ __device__ __forceinline__ void dsm_st(uint32_t a, uint32_t v)
 	asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
 }
 
-// Q-point column transforms of the columns q C/Q .. (q+1) C/Q - 1, all planes.
-template <int SET, int LQ, bool INV>
+// Q-point column transform of column j of plane PL (prime arithmetic z).
+template <int LQ, bool INV, class Z>
+__device__ __forceinline__ void cluster_col(const Z &z, uint32_t a, const uint32_t *fw, const uint32_t *iv)
+{
+	constexpr int Q = 1 << LQ;
+	uint32_t x[Q];
+#pragma unroll
+	for (int k = 0; k < Q; ++k) x[k] = dsm_ld(dsm_addr(a, k));
+	if constexpr (!INV) fwd_reg<Z, LQ>(z, x, 1u, fw);
+	else inv_reg<Z, LQ>(z, x, 1u, iv, true, __ldg(&fw[0]), __ldg(&iv[0]));
+#pragma unroll
+	for (int k = 0; k < Q; ++k) dsm_st(dsm_addr(a, k), x[k]);
+}
+
+// Q-point column transforms of the columns q C/Q .. (q+1) C/Q - 1, all planes
+// (plane-split shapes: a work item per (plane, column)).
+template <int SET, int LQ, int LC, bool INV>
 __device__ __forceinline__ void cluster_cols(uint32_t *sm, int q, const Tables &tab)
 {
-	using S = ClusterShape<LQ>;
+	using S = ClusterShape<LQ, LC>;
 	constexpr int Q = S::Q, CQ = S::C / Q;
-	using MP = RowMap<S::LC>;
+	using MP = RowMap<LC>;
 	const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
-#pragma unroll 1
-	for (int j = threadIdx.x; j < CQ; j += S::T)
+	if constexpr (S::PS)
 	{
-		const uint32_t off = base + 4u * static_cast<uint32_t>(MP::addr(q * CQ + j, 0));
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			using Z = ZS<SET, PL>;
-			const uint32_t a = off + 4u * PL * S::PC;
-			uint32_t x[Q];
-#pragma unroll
-			for (int k = 0; k < Q; ++k) x[k] = dsm_ld(dsm_addr(a, k));
-			if constexpr (!INV) fwd_reg<Z, LQ>(Z{}, x, 1u, tab.fw[PL]);
-			else inv_reg<Z, LQ>(Z{}, x, 1u, tab.iv[PL], true, __ldg(&tab.fw[PL][0]), __ldg(&tab.iv[PL][0]));
-#pragma unroll
-			for (int k = 0; k < Q; ++k) dsm_st(dsm_addr(a, k), x[k]);
-		});
+		constexpr int W = PrimeSet<SET>::W;
+#pragma unroll 1
+		for (int it = threadIdx.x; it < W * CQ; it += blockDim.x)
+		{
+			const int pl = it / CQ, j = it % CQ;
+			const auto z = prime_rt<SET>(pl);
+			const uint32_t a = base + 4u * static_cast<uint32_t>(pl * S::PC + MP::addr(q * CQ + j, 0));
+			cluster_col<LQ, INV>(z, a, tab.fw[pl], tab.iv[pl]);
+		}
+	}
+	else
+	{
+#pragma unroll 1
+		for (int j = threadIdx.x; j < CQ; j += S::T)
+		{
+			const uint32_t off = base + 4u * static_cast<uint32_t>(MP::addr(q * CQ + j, 0));
+			for_planes<SET>([&](auto PLc) {
+				constexpr int PL = decltype(PLc)::value;
+				using Z = ZS<SET, PL>;
+				cluster_col<LQ, INV>(Z{}, off + 4u * PL * S::PC, tab.fw[PL], tab.iv[PL]);
+			});
+		}
 	}
 }
 
 // One test of prime set SET on this cluster: `count` squarings (fewer when
 // the exponent runs out), from register src to register dst.
-template <int SET, int LQ>
+template <int SET, int LQ, int LC>
 __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDesc &d, uint32_t *sm, int q)
 {
 	namespace cg = cooperative_groups;
-	using S = ClusterShape<LQ>;
-	constexpr int Q = S::Q, C = S::C, PC = S::PC, T = S::T, D = S::D, W = PrimeSet<SET>::W;
-	using MP = RowMap<S::LC>;
+	using S = ClusterShape<LQ, LC>;
+	constexpr int Q = S::Q, C = S::C, PC = S::PC, T0 = S::T0, D = S::D, W = PrimeSet<SET>::W;
+	using MP = RowMap<LC>;
 	int64_t *const sc = reinterpret_cast<int64_t *>(sm + WMAX * PC);
 	cg::cluster_group cl = cg::this_cluster();
 	const int tid = threadIdx.x;
+	const bool owner = (tid < T0);
 	const Tables &tab = a.tab[SET];
 	const size_t N = size_t(C) * Q;
 	const size_t nseg = N / SEG;
@@ -595,6 +631,7 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 	if (a.dup_mode == DUP_BITS) iters = (pos0 + 1 < iters) ? static_cast<int>((pos0 < 0) ? 0 : pos0 + 1) : iters;
 
 	int32_t dg[D];
+	if (owner)
 	{
 		const size_t j0 = static_cast<size_t>(q) * C + static_cast<size_t>(tid) * D;
 		const int4 *src = reinterpret_cast<const int4 *>(d.regs + static_cast<size_t>(a.src) * N + j0);
@@ -604,7 +641,7 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 			const int4 v = src[i];
 			dg[4 * i] = v.x; dg[4 * i + 1] = v.y; dg[4 * i + 2] = v.z; dg[4 * i + 3] = v.w;
 		}
-		if (a.fix)
+		if (a.fix && (j0 % SEG == 0))
 		{
 			const int64_t cin = take_carry(d, j0 / SEG, nseg);
 			if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
@@ -614,43 +651,53 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 	for (int it = 0; it < iters; ++it)
 	{
 		const bool dup = (a.dup_mode == DUP_BITS) ? exp_bit(d.ebits, pos0 - it) : (a.dup_mode == DUP_ALL);
-		for_planes<SET>([&](auto PLc) {
-			constexpr int PL = decltype(PLc)::value;
-			using Z = ZS<SET, PL>;
-#pragma unroll
-			for (int i = 0; i < D; ++i) sm[PL * PC + MP::addr(tid * D + i, 0)] = Z::from_int(dg[i]);
-		});
-		cl.sync();
-		cluster_cols<SET, LQ, false>(sm, q, tab);
-		cl.sync();
-		row_core<SET, S::LC, MP>(sm, PC, 0, (1u << LQ) + static_cast<uint32_t>(q), tab, nullptr, 0, OP_SQUARE);
-		cl.sync();
-		cluster_cols<SET, LQ, true>(sm, q, tab);
-		cl.sync();
-		int64_t c = 0;
-#pragma unroll
-		for (int i = 0; i < D; ++i)
+		if (owner)
 		{
-			uint32_t x[3];
+			for_planes<SET>([&](auto PLc) {
+				constexpr int PL = decltype(PLc)::value;
+				using Z = ZS<SET, PL>;
 #pragma unroll
-			for (int pl = 0; pl < W; ++pl) x[pl] = sm[pl * PC + MP::addr(tid * D + i, 0)];
-			dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
+				for (int i = 0; i < D; ++i) sm[PL * PC + MP::addr(tid * D + i, 0)] = Z::from_int(dg[i]);
+			});
 		}
-		sc[tid] = c;
 		cl.sync();
-		int64_t cin;
-		if (tid > 0) cin = sc[tid - 1];
-		else
+		cluster_cols<SET, LQ, LC, false>(sm, q, tab);
+		cl.sync();
+		row_core<SET, LC, MP, S::PS>(sm, PC, 0, (1u << LQ) + static_cast<uint32_t>(q), tab, nullptr, 0, OP_SQUARE);
+		cl.sync();
+		cluster_cols<SET, LQ, LC, true>(sm, q, tab);
+		cl.sync();
+		if (owner)
 		{
-			const uint32_t qp = (q == 0) ? Q - 1 : q - 1;
-			const uint32_t ra = dsm_addr(static_cast<uint32_t>(__cvta_generic_to_shared(sc + T - 1)), qp);
-			const uint64_t lo = dsm_ld(ra), hi = dsm_ld(ra + 4);
-			cin = static_cast<int64_t>(lo | (hi << 32));
-			if (q == 0) cin = -cin;
+			int64_t c = 0;
+#pragma unroll
+			for (int i = 0; i < D; ++i)
+			{
+				uint32_t x[3];
+#pragma unroll
+				for (int pl = 0; pl < W; ++pl) x[pl] = sm[pl * PC + MP::addr(tid * D + i, 0)];
+				dg[i] = crt_carry<SET>(x, dup ? 1 : 0, d.ck, c);
+			}
+			sc[tid] = c;
 		}
-		if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
+		cl.sync();
+		if (owner)
+		{
+			int64_t cin;
+			if (tid > 0) cin = sc[tid - 1];
+			else
+			{
+				const uint32_t qp = (q == 0) ? Q - 1 : q - 1;
+				const uint32_t ra = dsm_addr(static_cast<uint32_t>(__cvta_generic_to_shared(sc + T0 - 1)), qp);
+				const uint64_t lo = dsm_ld(ra), hi = dsm_ld(ra + 4);
+				cin = static_cast<int64_t>(lo | (hi << 32));
+				if (q == 0) cin = -cin;
+			}
+			if (!absorb<D>(dg, cin, d.ck)) atomicOr(a.err, 1u);
+		}
 	}
 
+	if (owner)
 	{
 		const size_t j0 = static_cast<size_t>(q) * C + static_cast<size_t>(tid) * D;
 		int4 *dst = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(a.dst) * N + j0);
@@ -662,12 +709,12 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 
 // Persistent grid of clusters over the tests a.tests[0 .. ntests-1], of
 // either prime set.
-template <int LQ>
-__global__ void __launch_bounds__(ClusterShape<LQ>::T, 2) k_cluster(const Args a, int ntests)
+template <int LQ, int LC>
+__global__ void __launch_bounds__(ClusterShape<LQ, LC>::T, ClusterShape<LQ, LC>::MINB) k_cluster(const Args a, int ntests)
 {
 	pdl_wait();
 	namespace cg = cooperative_groups;
-	using S = ClusterShape<LQ>;
+	using S = ClusterShape<LQ, LC>;
 	extern __shared__ __align__(16) uint32_t sm[];
 	cg::cluster_group cl = cg::this_cluster();
 	const int q = static_cast<int>(cl.block_rank());
@@ -676,7 +723,7 @@ __global__ void __launch_bounds__(ClusterShape<LQ>::T, 2) k_cluster(const Args a
 	{
 		const int t = a.tests[ti];
 		const TestDesc &d = a.desc[t];
-		if (d.set == 0) cluster_test<0, LQ>(a, t, d, sm, q); else cluster_test<1, LQ>(a, t, d, sm, q);
+		if (d.set == 0) cluster_test<0, LQ, LC>(a, t, d, sm, q); else cluster_test<1, LQ, LC>(a, t, d, sm, q);
 		// the next test's first shared-memory writes follow this barrier, after
 		// every CTA has read this test's last carries
 		cl.sync();
@@ -1121,6 +1168,105 @@ __global__ void __launch_bounds__(MIDR_THREADS, midr_min_blocks(LR2)) k_midr(con
 	if (d.set == 0) midr_body<0, LR2, INV>(a, d, m, pl, c);
 	else if (d.set == 1) midr_body<1, LR2, INV>(a, d, m, pl, c);
 	else midr_body<2, LR2, INV>(a, d, m, pl, c);
+}
+
+// The 64-point middle pass (lr2 = 6) on thread pairs: lanes 2c' and 2c' + 1 of a
+// warp share column c of one plane of one block, 32 words each, so that a
+// thread holds what the 32-point pass holds (four CTAs per SM in 128
+// registers) instead of 64 words and their roots.  Forward: half h loads the
+// rows 16 h .. 16 h + 15 and 32 + 16 h .. 32 + 16 h + 15, whose first-stage
+// butterflies (rows j, j + 32) it then owns, and after that stage swaps 16
+// words with its partner so that it holds the rows 32 h .. 32 h + 31, on which
+// stages 1 .. 5 are the 32-point transform of base 2 base + h.  Inverse: the
+// same steps in reverse order.  The same butterflies with the same roots as
+// k_midr<6>, so the results are identical.  blockIdx.x = (m P + plane)
+// (C / MIDP_COLS) + chunk of MIDP_COLS columns.
+constexpr int MIDP_THREADS = 128;
+constexpr int MIDP_COLS = MIDP_THREADS / 2;
+constexpr int MIDP_COLS_LOG = 6;
+
+template <int SET, bool INV>
+__device__ __forceinline__ void midp_body(const Args &a, const TestDesc &d, int m, int pl, size_t c, int h)
+{
+	if (pl >= PrimeSet<SET>::W) return;
+	constexpr int LR2 = 6;
+	const int lc = a.n - MID_LR1 - LR2;
+	const size_t N = size_t(1) << a.n, C = size_t(1) << lc;
+	uint32_t *p = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(pl) * N +
+				  ((static_cast<size_t>(m) << LR2) << lc) + c;
+	const auto z = prime_rt<SET>(pl);
+	using Z = decltype(z);
+	const uint32_t base = (1u << MID_LR1) + static_cast<uint32_t>(m);
+	uint32_t x[32];
+	if constexpr (!INV)
+	{
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+		{
+			x[i] = p[static_cast<size_t>(16 * h + i) * C];
+			x[16 + i] = p[static_cast<size_t>(32 + 16 * h + i) * C];
+		}
+		typename Z::root_t w0[1];
+		load_twiddles<1>(w0, base, a.tab[SET].fw[pl]);
+#pragma unroll
+		for (int i = 0; i < 16; ++i) bfly_ct(z, x[i], x[16 + i], w0[0]);
+		// h = 0 keeps rows 0..15 and takes 16..31; h = 1 keeps 48..63 and takes 32..47
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+		{
+			const uint32_t send = h ? x[i] : x[16 + i];
+			const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, 1);
+			if (h) x[i] = recv; else x[16 + i] = recv;
+		}
+		fwd_thread<Z, 5>(z, x, 2u * base + static_cast<uint32_t>(h), a.tab[SET].fw[pl]);
+#pragma unroll
+		for (int i = 0; i < 32; ++i) p[static_cast<size_t>(32 * h + i) * C] = x[i];
+	}
+	else
+	{
+#pragma unroll
+		for (int i = 0; i < 32; ++i) x[i] = p[static_cast<size_t>(32 * h + i) * C];
+		inv_thread<Z, 5>(z, x, 2u * base + static_cast<uint32_t>(h), a.tab[SET].iv[pl]);
+		// back to the pairs of the first stage: h = 0 holds rows 0..15 with
+		// 32..47, h = 1 rows 16..31 with 48..63
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+		{
+			const uint32_t send = h ? x[i] : x[16 + i];
+			const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, 1);
+			if (h) x[i] = recv; else x[16 + i] = recv;
+		}
+		typename Z::root_t w0[1];
+		load_twiddles<1>(w0, base, a.tab[SET].iv[pl]);
+#pragma unroll
+		for (int i = 0; i < 16; ++i) bfly_gs(z, x[i], x[16 + i], w0[0]);
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+		{
+			p[static_cast<size_t>(16 * h + i) * C] = x[i];
+			p[static_cast<size_t>(32 + 16 * h + i) * C] = x[16 + i];
+		}
+	}
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(MIDP_THREADS, 4) k_midp(const Args a)
+{
+	pdl_wait();
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	const int chunks_log = a.n - MID_LR1 - 6 - MIDP_COLS_LOG;
+	const int P = static_cast<int>(gridDim.x >> (MID_LR1 + chunks_log));
+	const int q = static_cast<int>(blockIdx.x >> chunks_log);
+	const int m = q / P, pl = q % P;
+	const int h = static_cast<int>(threadIdx.x & 1);
+	const size_t c = (static_cast<size_t>(blockIdx.x & ((1u << chunks_log) - 1)) << MIDP_COLS_LOG) + (threadIdx.x >> 1);
+	if (d.set == 0) midp_body<0, INV>(a, d, m, pl, c, h);
+	else if (d.set == 1) midp_body<1, INV>(a, d, m, pl, c, h);
+	else midp_body<2, INV>(a, d, m, pl, c, h);
 }
 
 // ---- four-step with R <= 16 rows: one thread owns a whole column.
@@ -1821,6 +1967,63 @@ __global__ void k_copy(const Args a)
 	int4 *o = reinterpret_cast<int4 *>(a.desc[t].regs + static_cast<size_t>(a.dst) * N);
 	for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N / 4; i += size_t(gridDim.x) * blockDim.x)
 		o[i] = s[i];
+}
+
+// Root tables of one prime p for length N = 2^n, in the layout load_twiddles
+// reads (gf_ntt.cuh): entry k >= 1 of fw is psi^e and of iv is psi^-e, with
+// e = bitrev_n(k) and psi a primitive 2N-th root of unity; one word per entry
+// in Montgomery form (words = 1, the 32-bit primes) or the root in normal form
+// followed by its Shoup quotient floor(w 2^32 / p) (words = 2).  A thread
+// walks `run` consecutive exponents e, one product by psi (and by psi^-1) per
+// entry, and writes entry bitrev_n(e).  Entry 0 holds the normalisation
+// constants c (fw) and k0 (iv) computed by the host.  Exact integer
+// arithmetic: the same words as a host-side build.
+__device__ __forceinline__ uint32_t mulmod_u64(uint32_t a, uint32_t b, uint32_t p)
+{
+	return static_cast<uint32_t>((static_cast<uint64_t>(a) * b) % p);
+}
+
+__device__ __forceinline__ void put_root_d(uint32_t *t, uint32_t k, uint32_t w, uint32_t p, int words)
+{
+	if (words == 1) t[k] = static_cast<uint32_t>((static_cast<uint64_t>(w) << 32) % p);
+	else
+	{
+		t[2 * k] = w;
+		t[2 * k + 1] = static_cast<uint32_t>((static_cast<uint64_t>(w) << 32) / p);
+	}
+}
+
+__global__ void k_roots(uint32_t *fw, uint32_t *iv, uint32_t p, uint32_t psi, uint32_t psi_inv, int n, int words, int run,
+						uint32_t c, uint32_t k0)
+{
+	const uint32_t N = 1u << n;
+	const uint32_t e0 = (blockIdx.x * blockDim.x + threadIdx.x) * static_cast<uint32_t>(run);
+	if (e0 >= N) return;
+	// psi^e0 and psi^-e0 by square-and-multiply
+	uint32_t w = 1, wi = 1, y = psi, yi = psi_inv;
+	for (uint32_t e = e0; e != 0; e >>= 1)
+	{
+		if (e & 1) { w = mulmod_u64(w, y, p); wi = mulmod_u64(wi, yi, p); }
+		y = mulmod_u64(y, y, p);
+		yi = mulmod_u64(yi, yi, p);
+	}
+	for (uint32_t e = e0; (e < e0 + static_cast<uint32_t>(run)) && (e < N); ++e)
+	{
+		if (e == 0)
+		{
+			fw[0] = c;
+			iv[0] = k0;
+			if (words == 2) { fw[1] = 0; iv[1] = 0; }
+		}
+		else
+		{
+			const uint32_t k = __brev(e) >> (32 - n);
+			put_root_d(fw, k, w, p, words);
+			put_root_d(iv, k, wi, p, words);
+		}
+		w = mulmod_u64(w, psi, p);
+		wi = mulmod_u64(wi, psi_inv, p);
+	}
 }
 
 // pos[t] = max(pos[t] - count, -1) for every test (end of a four-step block;

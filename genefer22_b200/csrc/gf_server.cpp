@@ -15,6 +15,7 @@ namespace gfs {
 namespace {
 
 constexpr uint32_t NUM_REGS = 3;
+constexpr int OPENERS = 4;     // helper threads that open pools and checkers
 
 }  // namespace
 
@@ -76,7 +77,7 @@ Server::Server(const gfc_server_config &cfg, std::unique_ptr<Devices> dev)
 	: cfg_(cfg), dev_(std::move(dev)), t0_(std::chrono::steady_clock::now())
 {
 	if (cfg_.block == 0) throw Error{ GFC_ERR_ARG, "server: block length must be >= 1" };
-	opener_ = std::thread([this] { opener(); });
+	for (int i = 0; i < OPENERS; ++i) openers_.emplace_back([this] { opener(); });
 	thread_ = std::thread([this] { loop(); });
 }
 
@@ -89,7 +90,8 @@ Server::~Server()
 		open_jobs_.clear();
 	}
 	op_cv_.notify_all();
-	if (opener_.joinable()) opener_.join();
+	for (std::thread &t : openers_)
+		if (t.joinable()) t.join();
 }
 
 double Server::clock() const
@@ -152,6 +154,9 @@ void Server::info(gfc_server_stats *out)
 	out->used_bytes = used_;
 	out->budget_bytes = cfg_.budget_bytes;
 	out->gl_failures = gl_failures_;
+	out->open_s_sum = open_s_sum_;
+	out->open_s_max = open_s_max_;
+	out->step_s_max = step_s_max_;
 	out->pools_open = pools_open_;
 }
 
@@ -205,6 +210,7 @@ void Server::opener()
 			job = open_jobs_.front();
 			open_jobs_.pop_front();
 		}
+		const double t_open = clock();
 		try
 		{
 			if (job.pool != nullptr)
@@ -225,6 +231,12 @@ void Server::opener()
 				std::lock_guard<std::mutex> l(op_mu_);
 				opened_checks_.emplace_back(job.n, std::move(c));
 			}
+			{
+				const double dt = clock() - t_open;
+				std::lock_guard<std::mutex> l(out_mu_);
+				open_s_sum_ += dt;
+				open_s_max_ = std::max(open_s_max_, dt);
+			}
 		}
 		catch (const Error &e) { fail_loop(e.code, e.msg); }
 		catch (const std::exception &e) { fail_loop(GFC_ERR_CUDA, e.what()); }
@@ -240,7 +252,14 @@ void Server::loop()
 		while (!stop_)
 		{
 			bool progress = false;
+			const double t_step = clock();
 			step(progress);
+			const double dt = clock() - t_step;
+			if (dt > step_s_max_)
+			{
+				std::lock_guard<std::mutex> l(out_mu_);
+				step_s_max_ = dt;
+			}
 			if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(50));
 		}
 	}
@@ -265,7 +284,8 @@ void Server::loop()
 		stop_ = true;
 	}
 	op_cv_.notify_all();
-	if (opener_.joinable()) opener_.join();
+	for (std::thread &t : openers_)
+		if (t.joinable()) t.join();
 	opened_pools_.clear();
 	opened_checks_.clear();
 	pools_.clear();
@@ -629,7 +649,7 @@ GFC_API void gfc_server_default_config(gfc_server_config *cfg)
 	cfg->device = 0;
 	cfg->tune = 1;
 	cfg->keep_digits = 0;
-	cfg->idle_close_s = 0.25;
+	cfg->idle_close_s = 10.0;
 }
 
 GFC_API int gfc_server_create(const gfc_server_config *cfg, gfc_server **out)

@@ -15,7 +15,7 @@
 // Finished tests get genefer's Gerbicz-Li check (src/genefer.h:557-615),
 // several of one size at once, on a checker batch of their own.
 //
-// Pools are opened on a helper thread while the device-memory budget allows,
+// Pools are opened on helper threads while the device-memory budget allows,
 // and closed when idle.  The loop reaches the device only through the
 // Devices interface below: libgfcuda.so implements it with the engine's
 // batches (gf_server_cuda.cpp); a CPU build for the host-logic tests
@@ -86,7 +86,8 @@ struct CheckDev
 struct Devices
 {
 	virtual ~Devices() {}
-	// May run on the helper thread while the dispatcher drives other pools.
+	// May run on helper threads (several at once) while the dispatcher drives
+	// other pools.
 	virtual PoolDev *open_pool(uint32_t n, size_t capacity, uint32_t rep_b, uint32_t B, uint64_t max_bits, bool tune) = 0;
 	virtual CheckDev *open_check(uint32_t n, size_t group, uint32_t B) = 0;
 	// Whether the engine can run base b at size n at all, and whether b is in
@@ -158,7 +159,7 @@ private:
 		uint64_t bytes = 0;
 		bool packed_only = false;
 		uint32_t rep_b = 0;
-		std::unique_ptr<PoolDev> dev;      // null while the helper thread opens it
+		std::unique_ptr<PoolDev> dev;      // null while a helper thread opens it
 		std::vector<Slot> slots;
 		bool inflight = false;
 		double idle_since = 0;
@@ -209,8 +210,9 @@ private:
 	uint64_t used_ = 0, peak_ = 0;
 	std::map<uint32_t, int> tables_;            // pools + checkers holding each size's tables
 	uint64_t pools_created_ = 0, blocks_run_ = 0, gl_failures_ = 0;
+	double open_s_sum_ = 0, open_s_max_ = 0, step_s_max_ = 0;   // helper-thread opens, longest dispatcher step
 
-	// helper thread: opens pools and checkers
+	// helper threads: open pools and checkers
 	std::mutex op_mu_;
 	std::condition_variable op_cv_;
 	struct OpenJob
@@ -222,7 +224,7 @@ private:
 	std::deque<OpenJob> open_jobs_;
 	std::vector<std::pair<Pool *, std::unique_ptr<PoolDev>>> opened_pools_;
 	std::vector<std::pair<uint32_t, std::unique_ptr<CheckDev>>> opened_checks_;
-	std::thread opener_;
+	std::vector<std::thread> openers_;     // pools of different sizes open in parallel
 
 	// dispatcher -> poll
 	std::mutex out_mu_;

@@ -47,7 +47,10 @@ class TuneCache
 public:
 	void apply(gfc_batch *bt, uint32_t n, size_t cap, uint32_t rep_b)
 	{
-		const auto key = std::make_tuple(n, cap, gfc_width_for(rep_b, n), gfc_packed_range(rep_b, n));
+		// a pool of packed-range bases tunes with packed plans among the
+		// candidates, whatever the RNS width of its representative base
+		const int packed = gfc_packed_range(rep_b, n);
+		const auto key = std::make_tuple(n, cap, packed ? 4 : gfc_width_for(rep_b, n), packed);
 		{
 			std::lock_guard<std::mutex> l(mu_);
 			auto it = plans_.find(key);
@@ -65,15 +68,27 @@ private:
 	std::map<std::tuple<uint32_t, size_t, int, int>, int32_t> plans_;
 };
 
+// Pinned host buffers carved from a few large allocations (a pool asks for
+// two per slot; cudaHostAlloc per buffer made opening a wide pool slow).
 class PinnedBuffers
 {
 public:
 	int32_t *get(size_t count)
 	{
-		void *p = nullptr;
-		ckc(cudaHostAlloc(&p, count * sizeof(int32_t), cudaHostAllocDefault), "cudaHostAlloc");
-		bufs_.push_back(p);
-		return static_cast<int32_t *>(p);
+		const size_t bytes = (count * sizeof(int32_t) + 255) & ~size_t(255);
+		if (bytes > left_)
+		{
+			const size_t chunk = (bytes > (size_t(8) << 20)) ? bytes : (size_t(8) << 20);
+			void *p = nullptr;
+			ckc(cudaHostAlloc(&p, chunk, cudaHostAllocDefault), "cudaHostAlloc");
+			bufs_.push_back(p);
+			next_ = static_cast<char *>(p);
+			left_ = chunk;
+		}
+		int32_t *out = reinterpret_cast<int32_t *>(next_);
+		next_ += bytes;
+		left_ -= bytes;
+		return out;
 	}
 	~PinnedBuffers()
 	{
@@ -82,6 +97,8 @@ public:
 
 private:
 	std::vector<void *> bufs_;
+	char *next_ = nullptr;
+	size_t left_ = 0;
 };
 
 class CudaPool : public PoolDev

@@ -74,11 +74,15 @@ class MixedBatch:
         """Plan of each size class's pool (after ``run``)."""
         return dict(self._plans)
 
-    def run(self, validate: bool = True) -> List[Result]:
-        """Runs every test to the end of its exponent; results in job order."""
+    def run(self, validate: bool = True, warmup: bool = False) -> List[Result]:
+        """Runs every test to the end of its exponent; results in job order.
+        With ``warmup`` a first wave of one block per test opens the pools, and
+        the statistics cover the second wave only."""
         srv = Server(B=self.B, capacity=lambda n: self.counts.get(n, 1), tune=self.tune, validate=validate,
                      validate_group=4, keep_digits=True, device=self.device, idle_close_s=60.0)
-        comps = srv.run([Request(i, j, 0.0) for i, j in enumerate(self.jobs)])
+        warm = [Request(len(self.jobs) + i, Job.prefix(j.b, j.n, self.B), 0.0) for i, j in enumerate(self.jobs)] \
+            if warmup else []
+        comps = srv.run([Request(i, j, 0.0) for i, j in enumerate(self.jobs)], warmup=warm)
         st = srv.stats
         self.stats = MixedStats(seconds=max(c.residue_at for c in comps) - min(c.arrival for c in comps),
                                 digit_squarings=float(sum((1 << j.n) * j.nbits for j in self.jobs)))

@@ -142,6 +142,9 @@ class ServeStats:
     peak_bytes: int = 0
     budget_bytes: int = 0
     gl_failures: int = 0
+    open_s_sum: float = 0.0          # seconds the helper threads spent opening pools and checkers
+    open_s_max: float = 0.0
+    step_s_max: float = 0.0          # longest pass of the native dispatcher over its pools
     per_n: Dict[int, dict] = field(default_factory=dict)
 
     @property
@@ -161,7 +164,7 @@ class Server:
 
     def __init__(self, B: int = 1000, budget_bytes: int = 80 * 10**9,
                  capacity: Optional[Callable[[int], int]] = None, tune: bool = True, validate: bool = True,
-                 validate_group: int = 4, keep_digits: bool = False, device: int = 0, idle_close_s: float = 0.25,
+                 validate_group: int = 4, keep_digits: bool = False, device: int = 0, idle_close_s: float = 10.0,
                  lib=None):
         self.B = int(B)
         self.budget_bytes = int(budget_bytes)
@@ -193,9 +196,13 @@ class Server:
         cfg.idle_close_s = self.idle_close_s
         return cfg
 
-    def run(self, requests: Sequence[Request], timeout_s: float = 3600.0) -> List[Completion]:
+    def run(self, requests: Sequence[Request], timeout_s: float = 3600.0,
+            warmup: Sequence[Request] = ()) -> List[Completion]:
         """Serves ``requests`` (arrival times in seconds from the start of the
-        run) and returns their completions in request order."""
+        run) and returns their completions in request order.  ``warmup``
+        requests (ids distinct from the others) are served first, all at once,
+        and left out of the results and statistics: they open the pools, so
+        that the run measures the pools' steady state."""
         reqs = sorted(requests, key=lambda r: (r.arrival, r.id))
         L = self.L
         h = vp()
@@ -208,9 +215,22 @@ class Server:
                     reps = {1024} | {int(r.job.b) for r in reqs if int(r.job.n) == n and _packed_pool(r.job.b, n)}
                     for rep in sorted(reps)[:2]:
                         self._check(L.gfc_server_pretune(h, n, rep))
-            t0 = L.gfc_server_clock(h)
             buf = (CompletionC * 64)()
             got = ctypes.c_size_t(0)
+            if warmup:
+                for r in warmup:
+                    w = np.ascontiguousarray(r.job.words, dtype=np.uint32)
+                    self._check(L.gfc_server_submit(h, r.id, int(r.job.b), int(r.job.n),
+                                                    w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), int(r.job.nbits)))
+                left = len(warmup)
+                while left > 0:
+                    self._check(L.gfc_server_poll(h, buf, 64, ctypes.byref(got), 20))
+                    left -= got.value
+                    for i in range(got.value):
+                        if self.keep_digits:       # release the kept residue
+                            d = np.empty(1 << int(buf[i].n), dtype=np.int32)
+                            L.gfc_server_digits(h, buf[i].id, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), d.size)
+            t0 = L.gfc_server_clock(h)
             k = 0
             deadline = t0 + timeout_s
             while len(comps) < len(reqs):
@@ -248,7 +268,8 @@ class Server:
     def _summarise(self, reqs, cs: List[Completion], st: ServerStatsC):
         s = ServeStats(requests=len(reqs), completed=len(cs), pools_created=int(st.pools_created),
                        blocks_run=int(st.blocks_run), peak_bytes=int(st.peak_bytes), budget_bytes=int(st.budget_bytes),
-                       gl_failures=int(st.gl_failures))
+                       gl_failures=int(st.gl_failures), open_s_sum=float(st.open_s_sum),
+                       open_s_max=float(st.open_s_max), step_s_max=float(st.step_s_max))
         self.stats = s
         if not cs:
             return

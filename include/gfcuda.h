@@ -206,8 +206,9 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
 
 /* Kernel plan.  lr = 0: one CTA per test with the state in shared memory
  * (n <= 14); lr = 1: squarings by one thread-block cluster per test with the
- * state in the cluster's shared memory (15 <= n <= 17; products use the
- * default four-step plan); 3 <= lr <= 10: four-step with R = 2^lr rows
+ * state in the cluster's shared memory (12 <= n <= 17: eight CTAs with rows of
+ * 2^(n-3) up to n = 14, 2^(n-13) CTAs with rows of 2^13 above; products use the
+ * default plan of n); 3 <= lr <= 10: four-step with R = 2^lr rows
  * (8 <= n - lr <= 13); lr = 100 + lr2 (3 <= lr2 <= 7): six-step, the column
  * transform split into 2^4 and 2^lr2 points (8 <= n - 4 - lr2 <= 13);
  * lr = 200 + l (l = 3, 4): packed digits, two base-b digits per coefficient
@@ -331,10 +332,13 @@ typedef struct gfc_server_stats
 {
 	uint64_t submitted, completed, pools_created, pools_open, blocks_run;
 	uint64_t used_bytes, peak_bytes, budget_bytes, gl_failures;
+	double open_s_sum, open_s_max;   /* seconds spent opening pools and checkers (helper threads) */
+	double step_s_max;               /* longest pass of the dispatcher over its pools */
 } gfc_server_stats;
 
 /* block 1000, validate_group 4, budget 80 GB, default capacities, device 0,
- * tuning on, digits not kept, idle_close_s 0.25. */
+ * tuning on, digits not kept, idle_close_s 10 (a pool also closes at once
+ * when a waiting request of another size needs its memory). */
 void gfc_server_default_config(gfc_server_config *cfg);
 
 /* Starts the loop's threads; the server clock starts now. */

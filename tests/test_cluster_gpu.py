@@ -1,5 +1,6 @@
-"""Cluster-resident squaring (plan 1, 15 <= n <= 17): one thread-block cluster
-per test, the state in distributed shared memory across many squarings.
+"""Cluster-resident squaring (plan 1, 12 <= n <= 17): one thread-block cluster
+per test, the state in distributed shared memory across many squarings
+(eight CTAs with plane-split passes up to n = 14, rows of 2^13 above).
 Results must equal the oracle's (restated transformCPUi32) and the four-step
 plan's, digit for digit after canonicalisation."""
 import numpy as np
@@ -22,7 +23,7 @@ def rand_digits(rng, b, N):
     return rng.integers(-(b // 2), b // 2 + 1, size=N).astype(np.int32)
 
 
-@pytest.mark.parametrize("n", [15, 16, 17])
+@pytest.mark.parametrize("n", [12, 13, 14, 15, 16, 17])
 @pytest.mark.parametrize("b", [2_000_002, 1_999_999_998, 1024])
 def test_cluster_squarings_vs_oracle(oracle, n, b):
     rng = np.random.default_rng(n * 7 + b % 11)

@@ -53,7 +53,15 @@ LARGE_B = 2 * 10**9 - 2
 @pytest.mark.parametrize("n", [10, 11, 12, 13, 14])
 @pytest.mark.parametrize("b", [SMALL_B, LARGE_B])
 def test_single_cta_plan(oracle, n, b):
-    check_ops(oracle, b, n, seed=n)
+    check_ops(oracle, b, n, plan=0, seed=n)
+
+
+@pytest.mark.parametrize("n", [12, 13, 14])
+def test_lone_small_test_defaults_to_cluster(n):
+    """A lone test at n = 12..14 squares on the cluster plan (eight SMs) by
+    default, a wide batch on the single-CTA plan (one SM per test)."""
+    assert Transform(SMALL_B, n).batch.plan() == 1
+    assert Batch([SMALL_B] * 64, n).plan() == 0
 
 
 @pytest.mark.parametrize("n,lr", [(11, 3), (14, 3), (12, 4), (13, 5), (14, 6), (12, 3), (15, 3), (15, 7), (16, 4), (16, 8),

@@ -80,8 +80,8 @@ def test_serve_requests():
 
 
 def test_candidates():
-    assert candidates(12) == [0, 3, 4, 203]
-    assert candidates(14) == [0, 3, 4, 5, 6, 203, 204]
+    assert candidates(12) == [0, 1, 3, 4, 203]
+    assert candidates(14) == [0, 1, 3, 4, 5, 6, 203, 204]
     assert candidates(16) == [1, 3, 4, 5, 6, 7, 8, 203, 204, 103, 104]
     assert candidates(18) == [5, 6, 7, 8, 9, 10, 204, 303, 304, 305, 103, 104, 105, 106]
     assert candidates(23) == [10, 305, 306, 307, 106, 107]
