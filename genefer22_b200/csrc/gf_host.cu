@@ -631,13 +631,13 @@ bool plan_valid(int n, int lr)
 // candidate).  Without packed digits (single tests of 2 and 3 primes):
 // single-CTA up to n = 14, four-step with rows of 2^12 at n = 15, 16, then
 // six-step (16-point register column pass, register middle pass of 2^lr2
-// points) with lr2 = 3 for n = 17..19, 5 for n = 20, 21, 6 for n = 22 and 7 for
-// n = 23.
+// points) with lr2 = 3 for n = 17, 18, 4 for n = 19, 20, 5 for n = 21, 6 for
+// n = 22 and 7 for n = 23.
 int default_plan(int n)
 {
 	if (n <= SMALL_MAX_LOGN) return 0;
 	if (n <= 16) return n - 12;
-	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 3, 5, 5, 6, 7 };
+	static const int lr2[24] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 3, 4, 4, 5, 6, 7 };
 	return PLAN_SIX + lr2[n];
 }
 
@@ -646,6 +646,9 @@ int default_plan(int n)
 // one B200 against the fastest unpacked plan).
 size_t packed_min_tests(int n)
 {
+	// a lone n = 19 test: the unpacked six-step 104 (35.5 us per squaring) beats
+	// the packed 303 (39.4 us) since the 64-point middle pass runs on thread pairs
+	if (n == 19) return 2;
 	return (n >= 16) ? 1 : 0;
 }
 

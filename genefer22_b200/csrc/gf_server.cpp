@@ -203,12 +203,42 @@ void Server::opener()
 	for (;;)
 	{
 		OpenJob job;
+		std::unique_ptr<PoolDev> closing;
+		std::function<void()> host;
 		{
 			std::unique_lock<std::mutex> l(op_mu_);
-			op_cv_.wait(l, [&] { return !open_jobs_.empty() || stop_; });
-			if (open_jobs_.empty()) return;
-			job = open_jobs_.front();
-			open_jobs_.pop_front();
+			op_cv_.wait(l, [&] { return !open_jobs_.empty() || !close_jobs_.empty() || !host_jobs_.empty() || stop_; });
+			if (!host_jobs_.empty())
+			{
+				host = std::move(host_jobs_.front());
+				host_jobs_.pop_front();
+			}
+			else if (!close_jobs_.empty())
+			{
+				closing = std::move(close_jobs_.front());
+				close_jobs_.pop_front();
+			}
+			else
+			{
+				if (open_jobs_.empty()) return;
+				job = open_jobs_.front();
+				open_jobs_.pop_front();
+			}
+		}
+		if (host)
+		{
+			try { host(); }
+			catch (const Error &e) { fail_loop(e.code, e.msg); }
+			catch (const std::exception &e) { fail_loop(GFC_ERR_CUDA, e.what()); }
+			continue;
+		}
+		if (closing)
+		{
+			// releasing a pool frees device memory, which waits for the whole
+			// device: done here, not on the dispatcher thread
+			try { closing.reset(); }
+			catch (...) { }
+			continue;
 		}
 		const double t_open = clock();
 		try
@@ -241,6 +271,21 @@ void Server::opener()
 		catch (const Error &e) { fail_loop(e.code, e.msg); }
 		catch (const std::exception &e) { fail_loop(GFC_ERR_CUDA, e.what()); }
 	}
+}
+
+void Server::post_host(std::function<void()> f)
+{
+	{
+		std::lock_guard<std::mutex> l(op_mu_);
+		host_jobs_.push_back(std::move(f));
+	}
+	op_cv_.notify_one();
+}
+
+void Server::post_cont(std::function<void()> f)
+{
+	std::lock_guard<std::mutex> l(cont_mu_);
+	continuations_.push_back(std::move(f));
 }
 
 // ------------------------------------------------------------------ dispatcher
@@ -283,6 +328,7 @@ void Server::loop()
 		open_jobs_.clear();
 		stop_ = true;
 	}
+	// (helper threads release queued closed pools before they exit)
 	op_cv_.notify_all();
 	for (std::thread &t : openers_)
 		if (t.joinable()) t.join();
@@ -320,6 +366,14 @@ void Server::step(bool &progress)
 		}
 		opened_checks_.clear();
 	}
+	{
+		std::deque<std::function<void()>> conts;
+		{
+			std::lock_guard<std::mutex> l(cont_mu_);
+			conts.swap(continuations_);
+		}
+		for (auto &f : conts) { f(); progress = true; }
+	}
 	for (auto &p : pools_)
 		if (p->dev) service_pool(*p, progress);
 	place();
@@ -354,30 +408,42 @@ void Server::service_pool(Pool &p, bool &progress)
 	{
 		Slot &s = p.slots[i];
 		if ((s.state != READING) || !p.dev->read_done(i)) continue;
+		// the residue is on the host: copy it out of the slot's buffers, free the
+		// slot, and leave the canonical digits, res64 and the check's inputs to a
+		// helper thread
 		const size_t N = size_t(1) << p.n;
-		std::vector<int32_t> canon(s.x, s.x + N);
-		gfc_gint_unbalance(canon.data(), N, s.req.b);
-		uint64_t r64 = 0, o64 = 0;
-		s.comp.is_prp = gfc_gint_is_one(canon.data(), N, s.req.b, &r64, &o64);
-		s.comp.res64 = r64;
-		s.comp.old64 = o64;
-		s.comp.residue_at = clock();
-		if (cfg_.validate_group > 0)
+		const bool check = (cfg_.validate_group > 0);
+		auto f = std::make_shared<Finished>();
+		f->comp = s.comp;
+		f->comp.residue_at = clock();
+		f->x.assign(s.x, s.x + N);
+		if (check)
 		{
-			Finished f;
-			f.comp = s.comp;
-			f.x.assign(s.x, s.x + N);
-			f.d.assign(s.d, s.d + N);
-			f.res = chunk_sum(s.req.words.data(), s.req.nbits, cfg_.block, &f.res_bits);
-			checkers_[p.n].n = p.n;
-			checkers_[p.n].queue.push_back(std::move(f));
-			if (cfg_.keep_digits)
-			{
-				std::lock_guard<std::mutex> l(out_mu_);
-				digits_[s.comp.id] = std::move(canon);
-			}
+			f->d.assign(s.d, s.d + N);
+			f->res = chunk_sum(s.req.words.data(), s.req.nbits, cfg_.block, &f->res_bits);
 		}
-		else finish(s.comp, std::move(canon));
+		const uint32_t b = s.req.b, n = p.n;
+		post_host([this, f, b, n, check]() {
+			auto canon = std::make_shared<std::vector<int32_t>>(f->x);
+			gfc_gint_unbalance(canon->data(), canon->size(), b);
+			uint64_t r64 = 0, o64 = 0;
+			f->comp.is_prp = gfc_gint_is_one(canon->data(), canon->size(), b, &r64, &o64);
+			f->comp.res64 = r64;
+			f->comp.old64 = o64;
+			post_cont([this, f, canon, n, check]() {
+				if (check)
+				{
+					if (cfg_.keep_digits)
+					{
+						std::lock_guard<std::mutex> l(out_mu_);
+						digits_[f->comp.id] = std::move(*canon);
+					}
+					checkers_[n].n = n;
+					checkers_[n].queue.push_back(std::move(*f));
+				}
+				else finish(f->comp, std::move(*canon));
+			});
+		});
 		s.state = FREE;
 		s.req = Req();
 		progress = true;
@@ -468,7 +534,7 @@ void Server::place()
 			const uint64_t bytes = cap * (slot_bytes(n) + exponent_bytes(mb));
 			// the first pool of a size also brings the size's checker
 			const bool need_check = (cfg_.validate_group > 0) && (checkers_.count(n) == 0 || checkers_[n].bytes == 0);
-			const uint64_t cbytes = need_check ? cfg_.validate_group * (slot_bytes(n) + exponent_bytes(cfg_.block + 64)) : 0;
+			const uint64_t cbytes = need_check ? cfg_.validate_group * (slot_bytes(n) + exponent_bytes(cfg_.block + 96)) : 0;
 			if (!take_budget(n, bytes + cbytes))
 			{
 				bool any_pool = false;
@@ -519,25 +585,35 @@ void Server::service_checkers(bool &progress)
 		if (!c.dev) continue;
 		if (c.busy)
 		{
-			if (!c.dev->done()) continue;
-			std::vector<bool> ok;
-			c.dev->results(ok);
-			const double now = clock();
-			for (size_t i = 0; i < c.group.size(); ++i)
-			{
-				gfc_completion comp = c.group[i].comp;
-				comp.gl_ok = ok[i] ? 1 : 0;
-				comp.validated_at = now;
-				if (!ok[i])
-				{
-					std::lock_guard<std::mutex> l(out_mu_);
-					++gl_failures_;
-				}
-				finish(comp, {});
-			}
-			c.group.clear();
-			c.busy = false;
+			if (c.finishing || !c.dev->done()) continue;
+			// the hashes of the group's residues on a helper thread; the checker
+			// stays busy until its continuation has recorded them
+			c.finishing = true;
+			Checker *cp = &c;
+			post_host([this, cp]() {
+				auto ok = std::make_shared<std::vector<bool>>();
+				cp->dev->results(*ok);
+				post_cont([this, cp, ok]() {
+					const double now = clock();
+					for (size_t i = 0; i < cp->group.size(); ++i)
+					{
+						gfc_completion comp = cp->group[i].comp;
+						comp.gl_ok = (*ok)[i] ? 1 : 0;
+						comp.validated_at = now;
+						if (!(*ok)[i])
+						{
+							std::lock_guard<std::mutex> l(out_mu_);
+							++gl_failures_;
+						}
+						finish(comp, {});
+					}
+					cp->group.clear();
+					cp->busy = false;
+					cp->finishing = false;
+				});
+			});
 			progress = true;
+			continue;
 		}
 		if (c.queue.empty()) continue;
 		const size_t k = std::min<size_t>(c.queue.size(), cfg_.validate_group);
@@ -588,6 +664,11 @@ void Server::close_idle_pools()
 		if (!busy && !wanted && (starved || (now - p.idle_since > cfg_.idle_close_s)))
 		{
 			give_budget(p.n, p.bytes);
+			{
+				std::lock_guard<std::mutex> l(op_mu_);
+				close_jobs_.push_back(std::move(p.dev));
+			}
+			op_cv_.notify_all();
 			pools_.erase(pools_.begin() + static_cast<std::ptrdiff_t>(i));
 			std::lock_guard<std::mutex> l(out_mu_);
 			--pools_open_;

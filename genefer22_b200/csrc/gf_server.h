@@ -30,6 +30,7 @@
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -177,6 +178,7 @@ private:
 		uint64_t bytes = 0;
 		std::unique_ptr<CheckDev> dev;     // null until opened
 		bool opening = false, busy = false;
+		bool finishing = false;            // a helper thread is computing the group's results
 		std::deque<Finished> queue;
 		std::vector<Finished> group;
 	};
@@ -222,6 +224,16 @@ private:
 		uint64_t max_bits;
 	};
 	std::deque<OpenJob> open_jobs_;
+	std::deque<std::unique_ptr<PoolDev>> close_jobs_;   // closed pools, released by the helper threads
+	// Host work of the residues (canonical digits, res64, Gerbicz-Li hashes:
+	// seconds at n = 22, 23) runs on the helper threads; what it changes in
+	// the dispatcher's state it posts back as continuations, run by the
+	// dispatcher at its next pass.
+	std::deque<std::function<void()>> host_jobs_;
+	std::mutex cont_mu_;
+	std::deque<std::function<void()>> continuations_;
+	void post_host(std::function<void()> f);
+	void post_cont(std::function<void()> f);
 	std::vector<std::pair<Pool *, std::unique_ptr<PoolDev>>> opened_pools_;
 	std::vector<std::pair<uint32_t, std::unique_ptr<CheckDev>>> opened_checks_;
 	std::vector<std::thread> openers_;     // pools of different sizes open in parallel

@@ -191,22 +191,31 @@ private:
 class CudaCheck : public CheckDev
 {
 public:
-	CudaCheck(int device, uint32_t n, size_t group, uint32_t B) : device_(device), N_(size_t(1) << n), group_(group), B_(B)
+	// The check runs from one CUDA graph (recorded here, again after a change
+	// of prime set under the single-CTA plan): enqueued call by call it is
+	// thousands of launches at large n, whose queue would hold up the
+	// dispatcher thread until the device drained it.  Every exponent 2^res
+	// is padded to RB bits with leading zeros (squaring 1 keeps 1), so one
+	// graph serves every group.
+	CudaCheck(int device, uint32_t n, size_t group, uint32_t B)
+		: device_(device), N_(size_t(1) << n), group_(group), B_(B), RB_(B + 96)
 	{
 		ckc(cudaSetDevice(device), "cudaSetDevice");
 		std::vector<uint32_t> bases(group, 1024);
 		ck(gfc_batch_create(bases.data(), group, n, 3, device, nullptr, &bt_), "batch_create");
-		ck(gfc_batch_reserve(bt_, B + 96), "reserve");
+		ck(gfc_batch_reserve(bt_, RB_), "reserve");
 		stream_ = static_cast<cudaStream_t>(gfc_batch_stream(bt_));
 		ckc(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming), "cudaEventCreate");
 		for (auto *v : { &x_, &d_, &a_, &c_ })
 			for (size_t i = 0; i < group; ++i) v->push_back(pinned_.get(N_));
+		capture();
 	}
 
 	~CudaCheck() override
 	{
 		cudaSetDevice(device_);
 		if (ev_ != nullptr) { cudaEventSynchronize(ev_); cudaEventDestroy(ev_); }
+		if (g_ != nullptr) gfc_graph_destroy(g_);
 		if (bt_ != nullptr) gfc_batch_destroy(bt_);
 	}
 
@@ -216,34 +225,32 @@ public:
 	{
 		k_ = items.size();
 		b_.clear();
-		uint64_t rbits = 1;
-		for (const CheckItem &it : items) rbits = std::max(rbits, it.res_bits);
-		const std::vector<uint32_t> zero((rbits + 31) / 32, 0);
+		const std::vector<uint32_t> zero((RB_ + 31) / 32, 0);
 		for (size_t i = 0; i < group_; ++i)
 		{
 			if (i < k_)
 			{
-				std::vector<uint32_t> w((rbits + 31) / 32, 0);
+				if (items[i].res_bits > RB_) throw Error{ GFC_ERR_ARG, "check: exponent sum longer than the reserved bits" };
+				std::vector<uint32_t> w((RB_ + 31) / 32, 0);
 				std::copy(items[i].res.begin(), items[i].res.end(), w.begin());
-				ck(gfc_batch_admit(bt_, i, items[i].b, w.data(), rbits), "admit");
+				ck(gfc_batch_admit(bt_, i, items[i].b, w.data(), RB_), "admit");
 				std::memcpy(x_[i], items[i].x, N_ * sizeof(int32_t));
 				std::memcpy(d_[i], items[i].d, N_ * sizeof(int32_t));
 				ck(gfc_batch_set_async(bt_, i, 0, x_[i]), "set_async");
 				ck(gfc_batch_set_async(bt_, i, 1, d_[i]), "set_async");
 				b_.push_back(items[i].b);
 			}
-			else ck(gfc_batch_admit(bt_, i, 1024, zero.data(), rbits), "admit");
+			else ck(gfc_batch_admit(bt_, i, 1024, zero.data(), RB_), "admit");
 		}
-		ck(gfc_batch_init_multiplicand(bt_, 1), "init_multiplicand");
-		ck(gfc_batch_mul(bt_, 0), "mul");                  // d(t+1) = x d(t)
-		ck(gfc_batch_copy(bt_, 2, 0), "copy");
-		ck(gfc_batch_copy(bt_, 0, 1), "copy");
-		ck(gfc_batch_square(bt_, 0, B_), "square");         // d(t)^(2^B)
-		ck(gfc_batch_copy(bt_, 1, 0), "copy");
-		ck(gfc_batch_set(bt_, 1), "set");
-		ck(gfc_batch_square_exp(bt_, static_cast<uint32_t>(rbits)), "square_exp");   // 2^res
-		ck(gfc_batch_init_multiplicand(bt_, 1), "init_multiplicand");
-		ck(gfc_batch_mul(bt_, 0), "mul");
+		int rc = gfc_graph_launch(g_);
+		if (rc == GFC_ERR_STATE)
+		{
+			gfc_graph_destroy(g_);
+			g_ = nullptr;
+			capture();
+			rc = gfc_graph_launch(g_);
+		}
+		ck(rc, "graph_launch");
 		for (size_t i = 0; i < k_; ++i)
 		{
 			ck(gfc_batch_get_async(bt_, i, 0, a_[i]), "get_async");
@@ -266,10 +273,32 @@ public:
 	}
 
 private:
+	void capture()
+	{
+		ck(gfc_batch_capture_begin(bt_), "capture_begin");
+		int rc = gfc_batch_init_multiplicand(bt_, 1);
+		if (rc == GFC_OK) rc = gfc_batch_mul(bt_, 0);                 // d(t+1) = x d(t)
+		if (rc == GFC_OK) rc = gfc_batch_copy(bt_, 2, 0);
+		if (rc == GFC_OK) rc = gfc_batch_copy(bt_, 0, 1);
+		if (rc == GFC_OK) rc = gfc_batch_square(bt_, 0, B_);          // d(t)^(2^B)
+		if (rc == GFC_OK) rc = gfc_batch_copy(bt_, 1, 0);
+		if (rc == GFC_OK) rc = gfc_batch_set(bt_, 1);
+		if (rc == GFC_OK) rc = gfc_batch_square_exp(bt_, RB_);        // 2^res
+		if (rc == GFC_OK) rc = gfc_batch_init_multiplicand(bt_, 1);
+		if (rc == GFC_OK) rc = gfc_batch_mul(bt_, 0);
+		gfc_graph *g = nullptr;
+		const int rc2 = gfc_batch_capture_end(bt_, &g);
+		if ((rc != GFC_OK) && (g != nullptr)) gfc_graph_destroy(g);
+		ck(rc, "check sequence");
+		ck(rc2, "capture_end");
+		g_ = g;
+	}
+
 	int device_;
 	size_t N_, group_;
-	uint32_t B_;
+	uint32_t B_, RB_;
 	gfc_batch *bt_ = nullptr;
+	gfc_graph *g_ = nullptr;
 	cudaStream_t stream_ = nullptr;
 	cudaEvent_t ev_ = nullptr;
 	size_t k_ = 0;

@@ -220,8 +220,9 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
  * uses packed digits when every base is in the packed range (203 at n = 16,
  * 204 at n = 17, 18, 303 at n = 19, 20, 305 at n = 21, 22, 306 at n = 23);
  * otherwise single-CTA up to n = 14,
- * four-step at n = 15, 16 (lr = n - 12), six-step above (103 at n = 17..19,
- * 105 at n = 20, 21, 106 at n = 22, 107 at n = 23): the fastest plans measured
+ * four-step at n = 15, 16 (lr = n - 12), six-step above (103 at n = 17, 18,
+ * 104 at n = 19, 20, 105 at n = 21, 106 at n = 22, 107 at n = 23; a lone test at
+ * n = 19 too, packed or not, and at n = 12..14 the cluster plan): the fastest plans measured
  * on one B200.
  * gfc_batch_plan reads the current plan. */
 int gfc_batch_set_plan(gfc_batch *bt, int lr);

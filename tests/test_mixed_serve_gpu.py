@@ -156,7 +156,7 @@ def test_serve_alone_vs_mix(oracle):
     B = 32
     reqs = serve_requests(count=14, rate=200.0, blocks=[2, 3], B=B, seed=1005, ns=(15, 16, 17), big=None)
     ns = (15, 16, 17)
-    budget = (sum(2 * slot_bytes(n, B + 64) + table_bytes(n) for n in ns)   # checkers, root tables
+    budget = (sum(2 * slot_bytes(n, B + 96) + table_bytes(n) for n in ns)   # checkers, root tables
               + 2 * 2 * pool_slot_bytes(17, B))                               # two pools of two slots
     srv = Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True)
     comps = srv.run(reqs, timeout_s=600)

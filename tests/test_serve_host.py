@@ -166,7 +166,7 @@ def _requests(B, count=10, seed=5):
 
 def _budget(ns, cap, group, B):
     """Pools of `cap` slots for every size at once, their checkers and tables."""
-    return sum(cap * sv.pool_slot_bytes(n, B) + group * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
+    return sum(cap * sv.pool_slot_bytes(n, B) + group * sv.slot_bytes(n, B + 96) + sv.table_bytes(n) for n in ns)
 
 
 def test_serve_loop_on_oracle(fake_lib, oracle):
@@ -196,7 +196,7 @@ def test_serve_budget_rotates_pools(fake_lib, oracle):
     ns = sorted({r.job.n for r in reqs})
     assert len(ns) >= 2
     one = max(2 * sv.pool_slot_bytes(n, B) + sv.table_bytes(n) for n in ns)
-    checkers = sum(2 * sv.slot_bytes(n, B + 64) + sv.table_bytes(n) for n in ns)
+    checkers = sum(2 * sv.slot_bytes(n, B + 96) + sv.table_bytes(n) for n in ns)
     budget = one + checkers
     srv = sv.Server(B=B, budget_bytes=budget, capacity=lambda n: 2, validate_group=2, keep_digits=True,
                     idle_close_s=10.0, lib=fake_lib)
