@@ -470,7 +470,11 @@ def run_serve(args):
             "mean_queue_wait_s": st.mean_wait, "completed": st.completed, "gl_failures": st.gl_failures,
             "pools_created": st.pools_created, "blocks_run": st.blocks_run, "peak_budget_bytes": st.peak_bytes,
             "open_s_sum": st.open_s_sum, "open_s_max": st.open_s_max, "dispatcher_step_s_max": st.step_s_max,
-            "saturated_open_s": {"sum": cap.open_s_sum, "max": cap.open_s_max, "step_max": cap.step_s_max},
+            "dispatcher_phase_s_max": dict(zip(("continuations", "pools", "placing", "checks", "closing",
+                                                "pool_query", "pool_read", "pool_admit", "pool_launch"),
+                                               st.phase_s_max)),
+            "saturated_open_s": {"sum": cap.open_s_sum, "max": cap.open_s_max, "step_max": cap.step_s_max,
+                                 "phase_max": list(cap.phase_s_max)},
             "saturated": {"value": cap.rate, "seconds": cap.seconds, "p50_s": cap.p50, "p99_s": cap.p99},
             "per_n": {str(k): v for k, v in st.per_n.items()},
             "clocks": ck.summary()}

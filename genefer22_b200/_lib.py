@@ -41,7 +41,7 @@ class ServerStatsC(ctypes.Structure):
     """gfc_server_stats (include/gfcuda.h)."""
     _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "completed", "pools_created", "pools_open", "blocks_run",
                                                "used_bytes", "peak_bytes", "budget_bytes", "gl_failures")] + \
-        [(k, ctypes.c_double) for k in ("open_s_sum", "open_s_max", "step_s_max")]
+        [(k, ctypes.c_double) for k in ("open_s_sum", "open_s_max", "step_s_max")] + [("phase_s_max", ctypes.c_double * 9)]
 
 
 # The serving loop's entry points (also exported by the CPU build of the same

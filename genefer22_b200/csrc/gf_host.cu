@@ -433,7 +433,27 @@ void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 {
 	using S = RowShape<LC>;
 	const size_t smem = size_t(S::PC) * 4;          // one plane per CTA
-	if (prep) { set_smem(k_row<LC>, smem); return; }
+	if (prep) { set_smem(k_row<LC>, smem); set_smem(k_row2<LC>, 2 * smem); return; }
+	if ((planes == 4) && (a.op != OP_FWD) && (grid_y >= 2))
+	{
+		// packed batches: two tests per CTA sharing the row's roots (k_row2)
+		const dim3 grid((1u << (a.n - LC)) * 4u, static_cast<unsigned>((grid_y + 1) / 2));
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = grid;
+		cfg.blockDim = dim3(row_threads(LC));
+		cfg.dynamicSmemBytes = 2 * smem;
+		cfg.stream = s;
+		cudaLaunchAttribute at[1];
+		at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+		at[0].val.programmaticStreamSerializationAllowed = 1;
+		cfg.attrs = at;
+		cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+		GFC_CK(cudaStreamIsCapturing(s, &cs));
+		cfg.numAttrs = ((cs == cudaStreamCaptureStatusNone) || (a.pdl_graph != 0)) ? 1 : 0;
+		GFC_CK(cudaLaunchKernelEx(&cfg, k_row2<LC>, a, grid_y));
+		after_launch();
+		return;
+	}
 	const dim3 grid((1u << (a.n - LC)) * static_cast<unsigned>(planes), static_cast<unsigned>(grid_y));
 	launch_pdl(k_row<LC>, grid, dim3(row_threads(LC)), smem, s, a);
 }

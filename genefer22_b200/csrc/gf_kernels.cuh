@@ -360,6 +360,111 @@ __device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint
 	});
 }
 
+// One radix-2^r pass of a row of plane pl for two tests at once (k_row2):
+// the tests' tiles buf0, buf1 (or their rows in global memory g0, g1 for the
+// first forward and the last inverse pass), the same roots.  MODE as in
+// pass_all; lanes and plane splitting are not used.  `store1` false: the
+// second lane duplicates the first test and writes only its own tile.
+template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO>
+__device__ __forceinline__ void pass_pair(uint32_t *buf0, uint32_t *buf1, uint32_t base0, const Tables &tab,
+										  const uint32_t *__restrict__ zrow0, const uint32_t *__restrict__ zrow1,
+										  uint32_t *g0, uint32_t *g1, int pl, bool store1)
+{
+	constexpr int E = 1 << r;
+	constexpr int GL = L - r;
+	constexpr int STEP = 1 << (L - SIGMA - r);
+	const auto z = prime_rt<SET>(pl);
+	for (int g = threadIdx.x; g < (1 << GL); g += blockDim.x)
+	{
+		const Group G(g, L, SIGMA, r);
+		const uint32_t tb = (base0 << SIGMA) + G.blk;
+		const int base = Map::addr(G.i0, 0);
+		uint32_t x[E], y[E];
+		if constexpr (IO == IO_GIN)
+		{
+#pragma unroll
+			for (int m = 0; m < E; ++m) { x[m] = g0[G.i0 + m * STEP]; y[m] = g1[G.i0 + m * STEP]; }
+		}
+		else
+		{
+#pragma unroll
+			for (int m = 0; m < E; ++m) { x[m] = buf0[base + Map::off(m, STEP)]; y[m] = buf1[base + Map::off(m, STEP)]; }
+		}
+		if constexpr (MODE != PM_INV) fwd_reg2<decltype(z), r>(z, x, y, tb, tab.fw[pl]);
+		if constexpr (MODE == PM_MID_SQ)
+		{
+#pragma unroll
+			for (int m = 0; m < E; ++m) { x[m] = z.mul(x[m], x[m]); y[m] = z.mul(y[m], y[m]); }
+		}
+		if constexpr (MODE == PM_MID_MUL)
+		{
+#pragma unroll
+			for (int m = 0; m < E; ++m)
+			{
+				x[m] = z.mul(x[m], __ldg(&zrow0[G.i0 + m * STEP]));
+				y[m] = z.mul(y[m], __ldg(&zrow1[G.i0 + m * STEP]));
+			}
+		}
+		if constexpr (MODE != PM_FWD) inv_reg2<decltype(z), r>(z, x, y, tb, tab.iv[pl]);
+		if constexpr (IO == IO_GOUT)
+		{
+#pragma unroll
+			for (int m = 0; m < E; ++m) g0[G.i0 + m * STEP] = x[m];
+			if (store1)
+			{
+#pragma unroll
+				for (int m = 0; m < E; ++m) g1[G.i0 + m * STEP] = y[m];
+			}
+		}
+		else
+		{
+#pragma unroll
+			for (int m = 0; m < E; ++m) { buf0[base + Map::off(m, STEP)] = x[m]; buf1[base + Map::off(m, STEP)] = y[m]; }
+		}
+	}
+}
+
+// row_core_global for two tests (k_row2): squaring or product of row `base0`
+// of plane pl, the rows in global memory at g0, g1, tiles buf0, buf1.
+template <int SET, int L, class Map>
+__device__ __forceinline__ void row_core_pair(uint32_t *buf0, uint32_t *buf1, uint32_t base0, const Tables &tab,
+											  const uint32_t *zrow0, const uint32_t *zrow1, int op, uint32_t *g0,
+											  uint32_t *g1, int pl, bool store1)
+{
+	constexpr int NP = Sched<L>::NP;
+	static_assert(NP >= 2, "rows of at least two passes");
+	static_for<0, NP - 1>([&](auto P) {
+		constexpr int p = decltype(P)::value;
+		if constexpr (p == 0)
+			pass_pair<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map, IO_GIN>(buf0, buf1, base0, tab, nullptr, nullptr, g0, g1,
+																		   pl, store1);
+		else
+			pass_pair<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map, IO_SMEM>(buf0, buf1, base0, tab, nullptr, nullptr,
+																			nullptr, nullptr, pl, store1);
+		__syncthreads();
+	});
+	constexpr int PL = NP - 1;
+	if (op == OP_MUL)
+		pass_pair<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map, IO_SMEM>(buf0, buf1, base0, tab, zrow0, zrow1, nullptr,
+																			  nullptr, pl, store1);
+	else
+		pass_pair<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map, IO_SMEM>(buf0, buf1, base0, tab, nullptr, nullptr,
+																			 nullptr, nullptr, pl, store1);
+	__syncthreads();
+	static_for<0, NP - 1>([&](auto Q) {
+		constexpr int p = NP - 2 - decltype(Q)::value;
+		if constexpr (p == 0)
+			pass_pair<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_GOUT>(buf0, buf1, base0, tab, nullptr, nullptr, g0, g1,
+																			pl, store1);
+		else
+		{
+			pass_pair<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_SMEM>(buf0, buf1, base0, tab, nullptr, nullptr,
+																			nullptr, nullptr, pl, store1);
+			__syncthreads();
+		}
+	});
+}
+
 // Row transforms in shared memory: forward (OP_FWD), or forward + pointwise
 // square / product + inverse.
 template <int SET, int L, class Map, bool PSPLIT = false>
@@ -953,6 +1058,39 @@ __global__ void __launch_bounds__(row_threads(LC)) k_row(const Args a)
 	if (d.set == 0) row_body<0, LC>(a, d, sm);
 	else if (d.set == 1) row_body<1, LC>(a, d, sm);
 	else row_body<2, LC>(a, d, sm);
+}
+
+// Rows of packed-digit batches (every test on prime set 2), two tests per CTA:
+// blockIdx.x = row * 4 + plane, blockIdx.y = pair of the launch's tests.  The
+// tests' rows share their roots, which a thread loads once per group for
+// both, and the two tests' butterflies are independent chains.  Squarings and
+// products only (the forward transform of a multiplicand runs k_row).  A pair
+// with one test left (the other one past its exponent, or an odd count) runs
+// that test on both lanes and writes it once.
+__host__ __device__ constexpr int row2_min_blocks(int lc) { return (row_threads(lc) >= 512) ? 1 : 3; }
+
+template <int LC>
+__global__ void __launch_bounds__(row_threads(LC), row2_min_blocks(LC)) k_row2(const Args a, int ntests)
+{
+	pdl_wait();
+	extern __shared__ __align__(16) uint32_t sm[];
+	using S = RowShape<LC>;
+	const int i0 = 2 * static_cast<int>(blockIdx.y), i1 = i0 + 1;
+	int t0 = a.tests[i0], t1 = (i1 < ntests) ? a.tests[i1] : -1;
+	bool act0, act1 = (t1 >= 0);
+	(void)get_dup(a, a.desc[t0], t0, a.j, act0);
+	if (act1) (void)get_dup(a, a.desc[t1], t1, a.j, act1);
+	if (!act0 && !act1) return;
+	if (!act0) { t0 = t1; act1 = false; }
+	const bool store1 = act1;
+	if (!act1) t1 = t0;
+	const TestDesc &d0 = a.desc[t0], &d1 = a.desc[t1];
+	const int n = a.n, lr = n - LC;
+	const size_t N = size_t(1) << n;
+	const int k = static_cast<int>(blockIdx.x) >> 2, pl = static_cast<int>(blockIdx.x) & 3;
+	const size_t off = static_cast<size_t>(pl) * N + static_cast<size_t>(k) * S::C;
+	row_core_pair<2, LC, RowMap<LC>>(sm, sm + S::PC, (1u << lr) + static_cast<uint32_t>(k), a.tab[2],
+									 d0.zp + off, d1.zp + off, a.op, d0.planes + off, d1.planes + off, pl, store1);
 }
 
 // Columns: last log2 R inverse stages, CRT, carry inside 16-digit segments.

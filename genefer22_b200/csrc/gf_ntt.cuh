@@ -167,6 +167,51 @@ __device__ __forceinline__ void inv_reg(const Z &z, uint32_t (&x)[1 << r], uint3
 	});
 }
 
+// fwd_reg / inv_reg on two arrays that share their roots (the same row of two
+// tests): the roots are loaded once, and each stage's butterflies alternate
+// between the arrays, two independent chains.  No normalisation (rows never
+// contain global stage 0).
+template <class Z, int r>
+__device__ __forceinline__ void fwd_reg2(const Z &z, uint32_t (&x)[1 << r], uint32_t (&y)[1 << r], uint32_t tbase,
+										 const uint32_t *__restrict__ tw)
+{
+	typename Z::root_t w[(1 << r) - 1];
+	load_twiddles<r>(w, tbase, tw);
+#pragma unroll
+	for (int t = 0; t < r; ++t)
+	{
+		const int half = 1 << (r - 1 - t);
+#pragma unroll
+		for (int sb = 0; sb < (1 << t); ++sb)
+#pragma unroll
+			for (int m = 0; m < half; ++m)
+			{
+				bfly_ct(z, x[sb * 2 * half + m], x[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
+				bfly_ct(z, y[sb * 2 * half + m], y[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
+			}
+	}
+}
+
+template <class Z, int r>
+__device__ __forceinline__ void inv_reg2(const Z &z, uint32_t (&x)[1 << r], uint32_t (&y)[1 << r], uint32_t tbase,
+										 const uint32_t *__restrict__ twi)
+{
+	typename Z::root_t w[(1 << r) - 1];
+	load_twiddles<r>(w, tbase, twi);
+	static_for<0, r>([&](auto Q) {
+		constexpr int t = r - 1 - decltype(Q)::value;
+		constexpr int half = 1 << (r - 1 - t);
+#pragma unroll
+		for (int sb = 0; sb < (1 << t); ++sb)
+#pragma unroll
+			for (int m = 0; m < half; ++m)
+			{
+				bfly_gs(z, x[sb * 2 * half + m], x[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
+				bfly_gs(z, y[sb * 2 * half + m], y[sb * 2 * half + m + half], w[(1 << t) - 1 + sb]);
+			}
+	});
+}
+
 // Shared-memory address maps.  addr(i, lane) places element i of transform
 // `lane`; off(m, step) is the address offset of element i0 + m step from
 // element i0 for the groups the passes form (where it is independent of i0).

@@ -157,6 +157,7 @@ void Server::info(gfc_server_stats *out)
 	out->open_s_sum = open_s_sum_;
 	out->open_s_max = open_s_max_;
 	out->step_s_max = step_s_max_;
+	for (int k = 0; k < 9; ++k) out->phase_s_max[k] = phase_max_[k];
 	out->pools_open = pools_open_;
 }
 
@@ -366,6 +367,16 @@ void Server::step(bool &progress)
 		}
 		opened_checks_.clear();
 	}
+	double t = clock();
+	auto lap = [&](int k) {
+		const double now = clock();
+		if (now - t > phase_max_[k])
+		{
+			std::lock_guard<std::mutex> l(out_mu_);
+			phase_max_[k] = now - t;
+		}
+		t = now;
+	};
 	{
 		std::deque<std::function<void()>> conts;
 		{
@@ -374,11 +385,26 @@ void Server::step(bool &progress)
 		}
 		for (auto &f : conts) { f(); progress = true; }
 	}
+	lap(0);
 	for (auto &p : pools_)
 		if (p->dev) service_pool(*p, progress);
+	lap(1);
 	place();
+	lap(2);
 	service_checkers(progress);
+	lap(3);
 	close_idle_pools();
+	lap(4);
+}
+
+void Server::note_phase(int k, double t0)
+{
+	const double dt = clock() - t0;
+	if (dt > phase_max_[k])
+	{
+		std::lock_guard<std::mutex> l(out_mu_);
+		phase_max_[k] = dt;
+	}
 }
 
 void Server::service_pool(Pool &p, bool &progress)
@@ -386,7 +412,10 @@ void Server::service_pool(Pool &p, bool &progress)
 	const double now = clock();
 	if (p.inflight)
 	{
-		if (!p.dev->block_done()) return;
+		const double tq = clock();
+		const bool done = p.dev->block_done();
+		note_phase(5, tq);
+		if (!done) return;
 		p.inflight = false;
 		progress = true;
 		{
@@ -398,7 +427,9 @@ void Server::service_pool(Pool &p, bool &progress)
 			Slot &s = p.slots[i];
 			if ((s.state == ACTIVE) && (--s.blocks_left == 0))
 			{
+				const double tr = clock();
 				p.dev->read(i, s.x, s.d);
+				note_phase(6, tr);
 				s.state = READING;
 			}
 		}
@@ -463,7 +494,9 @@ void Server::service_pool(Pool &p, bool &progress)
 		const uint64_t pad = ((s.req.nbits + cfg_.block - 1) / cfg_.block) * cfg_.block;
 		std::vector<uint32_t> w((pad + 31) / 32, 0);
 		std::copy(s.req.words.begin(), s.req.words.end(), w.begin());
+		const double ta = clock();
 		p.dev->admit(i, s.req.b, w.data(), pad);
+		note_phase(7, ta);
 		s.blocks_left = pad / cfg_.block;
 		s.state = ACTIVE;
 		std::memset(&s.comp, 0, sizeof(s.comp));
@@ -481,7 +514,9 @@ void Server::service_pool(Pool &p, bool &progress)
 	for (const Slot &s : p.slots) active |= (s.state == ACTIVE);
 	if (active)
 	{
+		const double tl = clock();
 		p.dev->launch_block();
+		note_phase(8, tl);
 		p.inflight = true;
 		progress = true;
 		p.idle_since = now;

@@ -213,6 +213,10 @@ private:
 	std::map<uint32_t, int> tables_;            // pools + checkers holding each size's tables
 	uint64_t pools_created_ = 0, blocks_run_ = 0, gl_failures_ = 0;
 	double open_s_sum_ = 0, open_s_max_ = 0, step_s_max_ = 0;   // helper-thread opens, longest dispatcher step
+	// longest parts of a dispatcher pass: continuations, pools, placing, checks,
+	// closing; and of servicing a pool: event query, read-back, admission, block launch
+	double phase_max_[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+	void note_phase(int k, double t0);
 
 	// helper threads: open pools and checkers
 	std::mutex op_mu_;

@@ -145,6 +145,7 @@ class ServeStats:
     open_s_sum: float = 0.0          # seconds the helper threads spent opening pools and checkers
     open_s_max: float = 0.0
     step_s_max: float = 0.0          # longest pass of the native dispatcher over its pools
+    phase_s_max: tuple = ()          # its longest continuations / pools / placing / checks / closing parts
     per_n: Dict[int, dict] = field(default_factory=dict)
 
     @property
@@ -269,7 +270,8 @@ class Server:
         s = ServeStats(requests=len(reqs), completed=len(cs), pools_created=int(st.pools_created),
                        blocks_run=int(st.blocks_run), peak_bytes=int(st.peak_bytes), budget_bytes=int(st.budget_bytes),
                        gl_failures=int(st.gl_failures), open_s_sum=float(st.open_s_sum),
-                       open_s_max=float(st.open_s_max), step_s_max=float(st.step_s_max))
+                       open_s_max=float(st.open_s_max), step_s_max=float(st.step_s_max),
+                       phase_s_max=tuple(float(x) for x in st.phase_s_max))
         self.stats = s
         if not cs:
             return

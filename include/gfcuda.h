@@ -335,6 +335,8 @@ typedef struct gfc_server_stats
 	uint64_t used_bytes, peak_bytes, budget_bytes, gl_failures;
 	double open_s_sum, open_s_max;   /* seconds spent opening pools and checkers (helper threads) */
 	double step_s_max;               /* longest pass of the dispatcher over its pools */
+	double phase_s_max[9];           /* longest part of a pass: continuations, pools, placing, checks, closing;
+	                                    of servicing a pool: event query, read-back, admission, block launch */
 } gfc_server_stats;
 
 /* block 1000, validate_group 4, budget 80 GB, default capacities, device 0,
