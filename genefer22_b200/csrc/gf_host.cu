@@ -6,6 +6,7 @@
 // tests of one size class per launch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -152,6 +153,128 @@ void build_roots_device(uint32_t p, int n, uint32_t *fw, uint32_t *iv, cudaStrea
 	if (e != cudaSuccess) fail(GFC_ERR_CUDA, std::string("root table kernel: ") + cudaGetErrorString(e));
 }
 
+// ------------------------------------------------------------------ memory
+//
+// Device memory of batches and root tables comes from a stream-ordered pool
+// per device and goes back with cudaFreeAsync; pinned staging comes from a
+// cache of page-locked chunks.  cudaFree and cudaFreeHost wait for the whole
+// device, so a batch closed by one thread while others ran held every
+// thread's CUDA calls behind the work in flight on all streams, and pinning
+// fresh pages is slow.  Both keep freed memory for reuse up to a retention
+// limit: none by default, a server's budget while one runs.
+struct MemState
+{
+	std::mutex mu;
+	std::map<int, cudaMemPool_t> pools;
+	std::map<int, cudaStream_t> release;          // per device: frees of memory no work uses
+	std::map<void *, size_t> pinned;              // every live pinned chunk with its size
+	std::multimap<size_t, void *> pinned_free;    // cached chunks by size
+	size_t pinned_cached = 0;
+	size_t retain = 0;                            // bytes kept per device pool and in the pinned cache
+	int retainers = 0;
+};
+
+// Never destroyed: the CUDA runtime may be gone when static objects die.
+MemState &mem_state()
+{
+	static MemState *m = new MemState();
+	return *m;
+}
+
+size_t pinned_cap(const MemState &m) { return std::min(m.retain, size_t(32) << 30); }
+
+// The pool of the current device `device` (created on first use).
+cudaMemPool_t dev_pool(int device)
+{
+	MemState &m = mem_state();
+	std::lock_guard<std::mutex> l(m.mu);
+	auto it = m.pools.find(device);
+	if (it != m.pools.end()) return it->second;
+	cudaMemPoolProps pp{};
+	pp.allocType = cudaMemAllocationTypePinned;
+	pp.handleTypes = cudaMemHandleTypeNone;
+	pp.location.type = cudaMemLocationTypeDevice;
+	pp.location.id = device;
+	cudaMemPool_t pool = nullptr;
+	GFC_CK(cudaMemPoolCreate(&pool, &pp));
+	uint64_t keep = m.retain;
+	GFC_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+	cudaStream_t rs = nullptr;
+	GFC_CK(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
+	m.pools[device] = pool;
+	m.release[device] = rs;
+	return pool;
+}
+
+// Device memory ordered on stream s (usable elsewhere once s has synchronised).
+void *dev_alloc(int device, size_t bytes, cudaStream_t s)
+{
+	void *p = nullptr;
+	GFC_CK(cudaMallocFromPoolAsync(&p, bytes, dev_pool(device), s));
+	return p;
+}
+
+// Returns memory of dev_alloc that no queued or running work uses any more.
+void dev_free(int device, void *p)
+{
+	if (p == nullptr) return;
+	cudaStream_t rs = nullptr;
+	{
+		MemState &m = mem_state();
+		std::lock_guard<std::mutex> l(m.mu);
+		auto it = m.release.find(device);
+		if (it != m.release.end()) rs = it->second;
+	}
+	if (rs != nullptr) cudaFreeAsync(p, rs);
+}
+
+// Page-locked host memory of at least `bytes` (nullptr when CUDA refuses).
+void *pinned_get(size_t bytes)
+{
+	bytes = (bytes + 65535) & ~size_t(65535);
+	MemState &m = mem_state();
+	{
+		std::lock_guard<std::mutex> l(m.mu);
+		auto it = m.pinned_free.lower_bound(bytes);
+		if ((it != m.pinned_free.end()) && (it->first <= 2 * bytes))
+		{
+			void *p = it->second;
+			m.pinned_cached -= it->first;
+			m.pinned_free.erase(it);
+			return p;
+		}
+	}
+	void *p = nullptr;
+	if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess)
+	{
+		(void)cudaGetLastError();
+		return nullptr;
+	}
+	std::lock_guard<std::mutex> l(m.mu);
+	m.pinned[p] = bytes;
+	return p;
+}
+
+// Memory of pinned_get whose copies have all completed.
+void pinned_put(void *p)
+{
+	if (p == nullptr) return;
+	MemState &m = mem_state();
+	{
+		std::lock_guard<std::mutex> l(m.mu);
+		auto it = m.pinned.find(p);
+		if (it == m.pinned.end()) return;
+		if (m.pinned_cached + it->second <= pinned_cap(m))
+		{
+			m.pinned_free.emplace(it->second, p);
+			m.pinned_cached += it->second;
+			return;
+		}
+		m.pinned.erase(it);
+	}
+	cudaFreeHost(p);
+}
+
 // A private stream for building tables, synchronised and destroyed on scope exit.
 struct TableStream
 {
@@ -166,10 +289,8 @@ struct DeviceTables
 	int device = -1, n = 0;
 	uint32_t *d = nullptr;
 	Tables tab[3];
-	~DeviceTables()
-	{
-		if (d != nullptr) { cudaSetDevice(device); cudaFree(d); }
-	}
+	// every holder synchronised its stream before letting go of the tables
+	~DeviceTables() { dev_free(device, d); }
 };
 
 std::mutex g_tab_mu;
@@ -189,9 +310,9 @@ std::shared_ptr<DeviceTables> get_tables(int device, int n)
 	const size_t N = size_t(1) << n;
 	size_t off[5], total = 0;
 	for (int s = 0; s < 5; ++s) { off[s] = total; total += 2 * root_words(kPrime[s]) * N; }
-	GFC_CK(cudaMalloc(&t->d, total * sizeof(uint32_t)));
 	{
 		TableStream ts;
+		t->d = static_cast<uint32_t *>(dev_alloc(device, total * sizeof(uint32_t), ts.s));
 		for (int s = 0; s < 5; ++s)
 		{
 			const size_t words = root_words(kPrime[s]) * N;
@@ -238,9 +359,9 @@ std::shared_ptr<DeviceTables> get_tables_packed(int device, int np)
 	t->device = device; t->n = np;
 	const size_t N = size_t(1) << np;
 	const size_t words = 2 * N;                       // 31-bit primes: root and Shoup quotient
-	GFC_CK(cudaMalloc(&t->d, 8 * words * sizeof(uint32_t)));
 	{
 		TableStream ts;
+		t->d = static_cast<uint32_t *>(dev_alloc(device, 8 * words * sizeof(uint32_t), ts.s));
 		for (int pl = 0; pl < 4; ++pl)
 		{
 			t->tab[2].fw[pl] = t->d + (2 * pl) * words;
@@ -710,6 +831,7 @@ struct gfc_batch
 	int nset[2] = { 0, 0 }, offset[2] = { 0, 0 };   // tests per prime set; d_tests lists set 0 first
 	int pending = -1;             // register whose segment carries are not yet absorbed (four-step)
 	uint64_t sets_version = 0;    // bumped when a test changes prime set (per-set launches change)
+	bool tests_sorted = true;     // d_tests lists the tests by prime set (only the single-CTA plan needs it)
 	int cluster = 0;              // 1 when squarings use k_cluster (shape by n), else 0
 	int six = 0;                  // lr2 of a six-step plan (columns 2^4 x 2^lr2, lr = 4 + lr2), else 0
 	bool packed = false;          // prime set 2, two digits per coefficient, transform of N/2 (lr of that)
@@ -727,14 +849,17 @@ struct gfc_batch
 	size_t pin_slot = 0;          // bytes per slot in h_pin
 	std::vector<cudaEvent_t> slot_ev;   // recorded after a slot's staged copies were enqueued
 
+	// Waits for this batch's own stream only (not the device), then hands
+	// its memory and its hold on the root tables back.
 	~gfc_batch()
 	{
 		cudaSetDevice(device);
+		if (stream != nullptr) cudaStreamSynchronize(stream);
 		for (cudaEvent_t e : slot_ev) if (e != nullptr) cudaEventDestroy(e);
-		if (d_eres != nullptr) cudaFree(d_eres);
-		if (h_pin != nullptr) cudaFreeHost(h_pin);
-		for (uint32_t *e : ebits) if (e != nullptr) cudaFree(e);
-		if (mem != nullptr) cudaFree(mem);
+		dev_free(device, d_eres);
+		pinned_put(h_pin);
+		for (uint32_t *e : ebits) dev_free(device, e);
+		dev_free(device, mem);
 		if (own_stream && (stream != nullptr)) cudaStreamDestroy(stream);
 	}
 };
@@ -1188,7 +1313,7 @@ gfc_batch *batch_create(const uint32_t *b, size_t count, uint32_t n, size_t num_
 	const size_t s_car = al(count * (N / SEG) * 8 * PK_CARRY), s_desc = al(count * sizeof(TestDesc)), s_tests = al(count * 4);
 	const size_t s_pos = al(count * 8), s_err = 256;
 	bt->mem_bytes = s_regs + s_pl + s_zp + s_car + s_desc + s_tests + s_pos + s_err;
-	GFC_CK(cudaMalloc(&bt->mem, bt->mem_bytes));
+	bt->mem = dev_alloc(device, bt->mem_bytes, bt->stream);
 	char *p = static_cast<char *>(bt->mem);
 	bt->regs = reinterpret_cast<int32_t *>(p); p += s_regs;
 	bt->planes = reinterpret_cast<uint32_t *>(p); p += s_pl;
@@ -1376,11 +1501,10 @@ void op_reserve(gfc_batch &bt, uint64_t max_bits)
 	no_capture(bt);
 	const size_t words = (((max_bits + 31) / 32) + 3) & ~size_t(3);        // 16-byte multiple per slot
 	const size_t slot = (sizeof(TestDesc) + sizeof(int64_t) + 4 * words + 15) & ~size_t(15);
-	GFC_CK(cudaMalloc(&bt.d_eres, bt.count * words * sizeof(uint32_t)));
+	bt.d_eres = static_cast<uint32_t *>(dev_alloc(bt.device, bt.count * words * sizeof(uint32_t), bt.stream));
 	GFC_CK(cudaMemsetAsync(bt.d_eres, 0, bt.count * words * sizeof(uint32_t), bt.stream));
-	void *h = nullptr;
-	GFC_CK(cudaHostAlloc(&h, bt.count * slot + (bt.count + 1) * sizeof(int32_t), cudaHostAllocDefault));
-	bt.h_pin = static_cast<char *>(h);
+	bt.h_pin = static_cast<char *>(pinned_get(bt.count * slot + (bt.count + 1) * sizeof(int32_t)));
+	if (bt.h_pin == nullptr) fail(GFC_ERR_CUDA, "reserve: no page-locked host memory for the staging");
 	bt.res_words = words;
 	bt.pin_slot = slot;
 	*pin_one(bt) = 1;
@@ -1433,15 +1557,23 @@ void op_admit(gfc_batch &bt, size_t test, uint32_t b, const uint32_t *words, uin
 		bt.set[test] = s;
 		bt.nset[s]++;
 		bt.offset[0] = 0; bt.offset[1] = bt.nset[0];
-		staging_free(bt, bt.count);
-		int32_t *tl = pin_tests(bt);
-		size_t k = 0;
-		for (int q = 0; q < 2; ++q)
-			for (size_t i = 0; i < bt.count; ++i)
-				if (bt.set[i] == q) tl[k++] = static_cast<int32_t>(i);
-		GFC_CK(cudaMemcpyAsync(bt.d_tests, tl, bt.count * sizeof(int32_t), cudaMemcpyHostToDevice, bt.stream));
-		GFC_CK(cudaEventRecord(bt.slot_ev[bt.count], bt.stream));
-		if (bt.lr == 0) prepare_plan(bt);
+		if (bt.lr == 0)
+		{
+			// the per-set launches read the tests in prime-set order; the
+			// staging of the previous order is rewritten after its copy ran
+			// (a wait for the block in flight when two admissions of one
+			// window change sets)
+			staging_free(bt, bt.count);
+			int32_t *tl = pin_tests(bt);
+			size_t k = 0;
+			for (int q = 0; q < 2; ++q)
+				for (size_t i = 0; i < bt.count; ++i)
+					if (bt.set[i] == q) tl[k++] = static_cast<int32_t>(i);
+			GFC_CK(cudaMemcpyAsync(bt.d_tests, tl, bt.count * sizeof(int32_t), cudaMemcpyHostToDevice, bt.stream));
+			GFC_CK(cudaEventRecord(bt.slot_ev[bt.count], bt.stream));
+			prepare_plan(bt);
+		}
+		else bt.tests_sorted = false;   // every other launch covers all tests in any order
 	}
 	bt.b[test] = b;
 	TestDesc &d = bt.h_desc[test];
@@ -1471,6 +1603,15 @@ void set_plan_checked(gfc_batch &bt, int lr)
 	GFC_CK(cudaStreamSynchronize(bt.stream));
 	if (packed != bt.packed) set_packed(bt, packed);
 	apply_plan(bt, lr);
+	if ((bt.lr == 0) && !bt.tests_sorted)
+	{
+		std::vector<int32_t> tests;
+		for (int q = 0; q < 2; ++q)
+			for (size_t i = 0; i < bt.count; ++i)
+				if (bt.set[i] == q) tests.push_back(static_cast<int32_t>(i));
+		GFC_CK(cudaMemcpy(bt.d_tests, tests.data(), bt.count * sizeof(int32_t), cudaMemcpyHostToDevice));
+		bt.tests_sorted = true;
+	}
 	prepare_plan(bt);
 }
 
@@ -1506,6 +1647,42 @@ int guard(F &&f)
 // The message gfc_last_error returns on this thread, for the other sources of
 // the library (gf_server_cuda.cpp).
 void gfc_internal_set_error(const char *msg) { g_err = (msg != nullptr) ? msg : ""; }
+
+// Page-locked host memory from the library's cache (nullptr when CUDA
+// refuses), and its return once no copy uses it.
+void *gfc_internal_pinned_get(size_t bytes) { return pinned_get(bytes); }
+void gfc_internal_pinned_put(void *p) { pinned_put(p); }
+
+// A server keeps up to `bytes` of freed device memory in each device pool
+// and (at most 32 GB of) freed pinned memory for the pools it opens next;
+// when the last server ends, the pools and the cache give everything back.
+void gfc_internal_retain(bool on, size_t bytes)
+{
+	MemState &m = mem_state();
+	std::vector<void *> drop;
+	{
+		std::lock_guard<std::mutex> l(m.mu);
+		m.retainers += on ? 1 : -1;
+		if (m.retainers < 0) m.retainers = 0;
+		if (on) m.retain = std::max(m.retain, bytes);
+		else if (m.retainers == 0) m.retain = 0;
+		uint64_t keep = m.retain;
+		for (auto &pd : m.pools)
+		{
+			cudaMemPoolSetAttribute(pd.second, cudaMemPoolAttrReleaseThreshold, &keep);
+			if (keep == 0) cudaMemPoolTrimTo(pd.second, 0);
+		}
+		while (m.pinned_cached > pinned_cap(m))
+		{
+			auto it = std::prev(m.pinned_free.end());
+			m.pinned_cached -= it->first;
+			m.pinned.erase(it->second);
+			drop.push_back(it->second);
+			m.pinned_free.erase(it);
+		}
+	}
+	for (void *p : drop) cudaFreeHost(p);
+}
 
 GFC_API const char *gfc_last_error(void) { return g_err.c_str(); }
 GFC_API int gfc_version(void) { return 100; }
@@ -1669,13 +1846,15 @@ GFC_API int gfc_batch_set_exponent(gfc_batch *bt, size_t test, const uint32_t *w
 		}
 		GFC_CK(cudaStreamSynchronize(bt->stream));
 		const size_t nw = (nbits + 31) / 32;
-		if (bt->ebits[test] != nullptr) { GFC_CK(cudaFree(bt->ebits[test])); bt->ebits[test] = nullptr; }
-		GFC_CK(cudaMalloc(&bt->ebits[test], nw * sizeof(uint32_t)));
-		GFC_CK(cudaMemcpy(bt->ebits[test], words, nw * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		dev_free(bt->device, bt->ebits[test]);
+		bt->ebits[test] = nullptr;
+		bt->ebits[test] = static_cast<uint32_t *>(dev_alloc(bt->device, nw * sizeof(uint32_t), bt->stream));
 		bt->h_desc[test].ebits = bt->ebits[test];
-		GFC_CK(cudaMemcpy(bt->d_desc + test, &bt->h_desc[test], sizeof(TestDesc), cudaMemcpyHostToDevice));
 		const int64_t pos = static_cast<int64_t>(nbits) - 1;
-		GFC_CK(cudaMemcpy(bt->d_pos + test, &pos, sizeof(pos), cudaMemcpyHostToDevice));
+		GFC_CK(cudaMemcpyAsync(bt->ebits[test], words, nw * sizeof(uint32_t), cudaMemcpyHostToDevice, bt->stream));
+		GFC_CK(cudaMemcpyAsync(bt->d_desc + test, &bt->h_desc[test], sizeof(TestDesc), cudaMemcpyHostToDevice, bt->stream));
+		GFC_CK(cudaMemcpyAsync(bt->d_pos + test, &pos, sizeof(pos), cudaMemcpyHostToDevice, bt->stream));
+		GFC_CK(cudaStreamSynchronize(bt->stream));
 	});
 }
 
@@ -1788,6 +1967,7 @@ GFC_API int gfc_batch_assign(gfc_batch *bt, size_t test, uint32_t b)
 		}
 		GFC_CK(cudaMemcpy(bt->d_desc + test, &d, sizeof(TestDesc), cudaMemcpyHostToDevice));
 		GFC_CK(cudaMemcpy(bt->d_tests, tests.data(), bt->count * sizeof(int32_t), cudaMemcpyHostToDevice));
+		bt->tests_sorted = true;
 		prepare_plan(*bt);
 	});
 }

@@ -17,6 +17,10 @@
 
 #include "gf_server.h"
 
+void *gfc_internal_pinned_get(size_t bytes);
+void gfc_internal_pinned_put(void *p);
+void gfc_internal_retain(bool on, size_t bytes);
+
 namespace gfs {
 
 namespace {
@@ -68,8 +72,10 @@ private:
 	std::map<std::tuple<uint32_t, size_t, int, int>, int32_t> plans_;
 };
 
-// Pinned host buffers carved from a few large allocations (a pool asks for
-// two per slot; cudaHostAlloc per buffer made opening a wide pool slow).
+// Pinned host buffers carved from a few large chunks of the library's pinned
+// cache (a pool asks for two per slot; a page-locked allocation per buffer
+// made opening a wide pool slow, and freeing one waits for the device).
+// The owner destroys them after its last copy completed.
 class PinnedBuffers
 {
 public:
@@ -79,8 +85,8 @@ public:
 		if (bytes > left_)
 		{
 			const size_t chunk = (bytes > (size_t(8) << 20)) ? bytes : (size_t(8) << 20);
-			void *p = nullptr;
-			ckc(cudaHostAlloc(&p, chunk, cudaHostAllocDefault), "cudaHostAlloc");
+			void *p = gfc_internal_pinned_get(chunk);
+			if (p == nullptr) throw Error{ GFC_ERR_CUDA, "no page-locked host memory for a pool's buffers" };
 			bufs_.push_back(p);
 			next_ = static_cast<char *>(p);
 			left_ = chunk;
@@ -92,7 +98,7 @@ public:
 	}
 	~PinnedBuffers()
 	{
-		for (void *p : bufs_) cudaFreeHost(p);
+		for (void *p : bufs_) gfc_internal_pinned_put(p);
 	}
 
 private:
@@ -310,7 +316,10 @@ private:
 class CudaDevices : public Devices
 {
 public:
-	explicit CudaDevices(int device) : device_(device) {}
+	// Freed device and pinned memory stays with the library for the next
+	// pools, up to the budget, while the server runs.
+	CudaDevices(int device, uint64_t budget) : device_(device) { gfc_internal_retain(true, budget); }
+	~CudaDevices() override { gfc_internal_retain(false, 0); }
 
 	PoolDev *open_pool(uint32_t n, size_t capacity, uint32_t rep_b, uint32_t B, uint64_t max_bits, bool tune) override
 	{
@@ -345,7 +354,7 @@ std::unique_ptr<Devices> make_devices(const gfc_server_config &cfg)
 	int ndev = 0;
 	ckc(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
 	if ((cfg.device < 0) || (cfg.device >= ndev)) throw Error{ GFC_ERR_ARG, "server: no such device" };
-	return std::unique_ptr<Devices>(new CudaDevices(cfg.device));
+	return std::unique_ptr<Devices>(new CudaDevices(cfg.device, cfg.budget_bytes));
 }
 
 }  // namespace gfs

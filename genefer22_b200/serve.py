@@ -291,6 +291,22 @@ class Server:
 
 # ------------------------------------------------------------------ the serving workload
 
+
+def warmup_requests(requests: Sequence[Request], B: int, first_id: int = 10**9) -> List[Request]:
+    """One single-block request per pool shape that ``requests`` open (size,
+    and packed-digit range from 2^19 on), arriving at once: served before a
+    run, they open the pools and checkers the run then finds warm."""
+    out: List[Request] = []
+    seen = set()
+    for r in requests:
+        key = (int(r.job.n), _packed_pool(r.job.b, r.job.n))
+        if key in seen:
+            continue
+        seen.add(key)
+        out.append(Request(first_id + len(out), Job.prefix(int(r.job.b), int(r.job.n), int(B)), 0.0))
+    return out
+
+
 SERVE_LIMITS = {15: 2_000_000_000, 16: 1_500_000_000, 17: 1_000_000_000, 18: 1_000_000_000,
                 19: 70_000_000, 20: 55_000_000, 21: 45_000_000, 22: 35_000_000, 23: 25_000_000}
 
