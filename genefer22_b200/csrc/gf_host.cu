@@ -284,13 +284,26 @@ struct TableStream
 	void sync() { GFC_CK(cudaStreamSynchronize(s)); }
 };
 
+// Twist factors of one six-step split (k_twist) for every prime of a table.
+struct TwistTables
+{
+	uint32_t *d = nullptr;
+	const uint32_t *tf[3][4] = {}, *ti[3][4] = {};
+};
+
 struct DeviceTables
 {
 	int device = -1, n = 0;
 	uint32_t *d = nullptr;
 	Tables tab[3];
+	std::mutex tw_mu;
+	std::map<int, TwistTables> twist;   // by log2 rows of the split, built on first use
 	// every holder synchronised its stream before letting go of the tables
-	~DeviceTables() { dev_free(device, d); }
+	~DeviceTables()
+	{
+		for (auto &t : twist) dev_free(device, t.second.d);
+		dev_free(device, d);
+	}
 };
 
 std::mutex g_tab_mu;
@@ -330,6 +343,60 @@ std::shared_ptr<DeviceTables> get_tables(int device, int n)
 		}
 	g_tab_cache[key] = t;
 	return t;
+}
+
+// The six-step twist factors of table t (2^t.n points, prime sets 0 and 1,
+// or set 2 when `packed`) for R = 2^lr rows, built on the device on first use.
+const TwistTables &get_twist(DeviceTables &t, bool packed, int lr)
+{
+	std::lock_guard<std::mutex> lock(t.tw_mu);
+	auto it = t.twist.find(lr);
+	if (it != t.twist.end()) return it->second;
+	const int n = t.n;
+	const size_t C = size_t(1) << (n - lr);
+	uint32_t primes[5];
+	int np = 0;
+	if (packed) for (int pl = 0; pl < 4; ++pl) primes[np++] = PrimeSet<2>::p[pl];
+	else for (int s = 0; s < 5; ++s) primes[np++] = kPrime[s];
+	size_t off[5], total = 0;
+	for (int k = 0; k < np; ++k) { off[k] = total; total += 2 * (16 + root_words(primes[k])) * C; }
+	TwistTables tw;
+	{
+		TableStream ts;
+		tw.d = static_cast<uint32_t *>(dev_alloc(t.device, total * sizeof(uint32_t), ts.s));
+		for (int k = 0; k < np; ++k)
+		{
+			const uint32_t p = primes[k], N = 1u << n;
+			const uint32_t psi = powmod_h(primitive_root(p), (p - 1) / (2ull * N), p);
+			const uint32_t psi_inv = powmod_h(psi, 2ull * N - 1, p);
+			const size_t words = (16 + root_words(p)) * C;
+			const unsigned blocks = static_cast<unsigned>((16 * C + 255) / 256);
+			k_twist<<<blocks, 256, 0, ts.s>>>(tw.d + off[k], tw.d + off[k] + words, p, psi, psi_inv, n, lr,
+											  static_cast<int>(root_words(p)));
+			const cudaError_t e = cudaGetLastError();
+			if (e != cudaSuccess)
+			{
+				ts.sync();
+				dev_free(t.device, tw.d);
+				fail(GFC_ERR_CUDA, std::string("twist table kernel: ") + cudaGetErrorString(e));
+			}
+		}
+		ts.sync();
+	}
+	for (int k = 0; k < np; ++k)
+	{
+		const size_t words = (16 + root_words(primes[k])) * C;
+		const int set = packed ? 2 : ((k < 2) ? 0 : 1), pl = packed ? k : ((k < 2) ? k : k - 2);
+		tw.tf[set][pl] = tw.d + off[k];
+		tw.ti[set][pl] = tw.d + off[k] + words;
+	}
+	if (!packed)
+	{
+		// set 0 has two planes; its plane 2 is unused (as in the root tables)
+		tw.tf[0][2] = tw.tf[0][1];
+		tw.ti[0][2] = tw.ti[0][1];
+	}
+	return t.twist.emplace(lr, tw).first->second;
 }
 
 // Exact range: with |digit| <= D = b/2 + 1 every coefficient of a product of
@@ -836,6 +903,7 @@ struct gfc_batch
 	int six = 0;                  // lr2 of a six-step plan (columns 2^4 x 2^lr2, lr = 4 + lr2), else 0
 	bool packed = false;          // prime set 2, two digits per coefficient, transform of N/2 (lr of that)
 	std::shared_ptr<DeviceTables> tabp;   // root tables of prime set 2 at length N/2
+	const TwistTables *twist = nullptr;   // six-step plans whose middle pass twists (lr2 <= 6)
 	int cluster_max = 0;          // clusters of k_cluster resident at once
 	bool capturing = false;
 	uint64_t capture_start = 0;   // launch counter at capture_begin
@@ -963,6 +1031,16 @@ Args make_args(const gfc_batch &bt)
 	a.tab[0] = bt.tab->tab[0];
 	a.tab[1] = bt.tab->tab[1];
 	if (bt.tabp) a.tab[2] = bt.tabp->tab[2];
+	if (bt.twist != nullptr)
+	{
+		a.twist = 1;
+		for (int st = 0; st < 3; ++st)
+			for (int pl = 0; pl < 4; ++pl)
+			{
+				a.tab[st].tf[pl] = bt.twist->tf[st][pl];
+				a.tab[st].ti[pl] = bt.twist->ti[st][pl];
+			}
+	}
 	a.n = bt.n;
 	a.lr = bt.lr;
 	a.num_regs = static_cast<int>(bt.num_regs);
@@ -989,8 +1067,32 @@ void launch_cluster(gfc_batch &bt, const Args &a, cudaStream_t s)
 }
 
 // Raises shared-memory limits of the kernels the current plan uses.
+// Whether a six-step plan twists in its middle pass (every row then reads
+// the same C - 1 roots): where one direction of the row-pass root tables
+// (32 B per point of the packed transform, 24 B per point with a test on
+// the three-prime set, else 8 B) reaches 32 MB, and only for the register
+// middle passes of 2^3 .. 2^5 rows.  (The tables of every prime are built,
+// so a later admission on another prime set stays exact.)  Measured per squaring on one
+// B200 (graph replay, twist off -> on): packed n = 21 plan 305 76.0 -> 73.6
+// us, n = 22 145.5 -> 138.0, n = 23 plan 305 315.8 -> 298.1; unpacked
+// n = 21 plan 105 104.7 -> 99.7; but packed n = 20 plan 303 42.4 -> 44.2
+// (its tables stay in L2) and the 64-row pair pass (k_midp, at its
+// register limit) 35 -> 47 us per launch at n = 23, more than the rows gain.
+bool twist_pays(const gfc_batch &bt)
+{
+	if ((bt.six < 3) || (bt.six > 5)) return false;
+	size_t per_point = 8;
+	if (bt.packed) per_point = 32;
+	else if (bt.nset[1] > 0) per_point = 24;
+	const size_t points = size_t(1) << (bt.packed ? bt.n - 1 : bt.n);
+	return per_point * points >= (size_t(32) << 20);
+}
+
 void prepare_plan(gfc_batch &bt)
 {
+	bt.twist = nullptr;
+	if (twist_pays(bt))
+		bt.twist = bt.packed ? &get_twist(*bt.tabp, true, bt.lr) : &get_twist(*bt.tab, false, bt.lr);
 	Args a{};
 	a.n = bt.n;
 	if (bt.cluster > 0) launch_cluster_n(bt.n, a, 0, 0, nullptr, true, &bt.cluster_max);

@@ -61,6 +61,8 @@ struct Tables
 {
 	const uint32_t *fw[4];  // forward roots
 	const uint32_t *iv[4];  // inverse roots
+	const uint32_t *tf[4];  // six-step twist factors, forward (twist_regs), of the batch's split
+	const uint32_t *ti[4];  // and inverse
 };
 
 struct Args
@@ -75,6 +77,7 @@ struct Args
 	int op, dup_mode, count, j;  // operation, dup source, squarings (k_small), squaring index in block
 	int fix;                // four-step column-forward: register src has pending segment carries
 	int pdl_graph;          // host only: graph-captured launches keep programmatic edges
+	int twist;              // six-step: the middle pass twists, every row transform has base 1
 };
 
 template <int SET, int PL>
@@ -215,7 +218,7 @@ struct Sched
 // consecutive groups, so each of its 2^r accesses is one coalesced line).
 enum : int { IO_SMEM = 0, IO_GIN = 1, IO_GOUT = 2 };
 
-template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO = IO_SMEM, bool PSPLIT = false>
+template <int SET, int r, int MODE, int L, int SIGMA, class Map, int IO = IO_SMEM, bool PSPLIT = false, bool NORM = true>
 __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										 uint32_t base_step, const Tables &tab, const uint32_t *__restrict__ zrow,
 										 size_t zstride, uint32_t *gmem = nullptr, size_t gstride = 0, int pl_lo = 0,
@@ -272,7 +275,8 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 				for (int m = 0; m < E; ++m) x[m] = z.mul(x[m], __ldg(&zz[m * STEP]));
 			}
 			if constexpr (MODE != PM_FWD)
-				inv_reg<decltype(z), r>(z, x, tb, tab.iv[pl], tb == 1u, __ldg(&tab.fw[pl][0]), __ldg(&tab.iv[pl][0]));
+				inv_reg<decltype(z), r>(z, x, tb, tab.iv[pl], NORM && (tb == 1u), __ldg(&tab.fw[pl][0]),
+										__ldg(&tab.iv[pl][0]));
 			if constexpr (IO == IO_GOUT)
 			{
 #pragma unroll
@@ -320,7 +324,9 @@ __device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_lo
 // Row transform of one row whose planes stay in global memory at g (plane
 // stride gstride): the first forward pass reads them, the last inverse pass
 // writes them, the passes between go through the shared-memory tile.
-// Squaring or product only (not OP_FWD).
+// Squaring or product only (not OP_FWD).  A row never holds global stage 0
+// (its base is R + k, or 1 after a six-step twist), so no inverse pass
+// normalises.
 template <int SET, int L, class Map>
 __device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint32_t base0, const Tables &tab,
 												const uint32_t *zrow, size_t zstride, int op, uint32_t *g, size_t gstride,
@@ -340,21 +346,21 @@ __device__ __forceinline__ void row_core_global(uint32_t *buf, int pstride, uint
 	});
 	constexpr int PL = NP - 1;
 	if (op == OP_MUL)
-		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride,
-																	nullptr, 0, pl_lo, pl_hi);
+		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map, IO_SMEM, false, false>(
+			buf, pstride, 0, false, base0, 1u, tab, zrow, zstride, nullptr, 0, pl_lo, pl_hi);
 	else
-		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map>(buf, pstride, 0, false, base0, 1u, tab, zrow, zstride,
-																   nullptr, 0, pl_lo, pl_hi);
+		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map, IO_SMEM, false, false>(
+			buf, pstride, 0, false, base0, 1u, tab, zrow, zstride, nullptr, 0, pl_lo, pl_hi);
 	__syncthreads();
 	static_for<0, NP - 1>([&](auto Q) {
 		constexpr int p = NP - 2 - decltype(Q)::value;
 		if constexpr (p == 0)
-			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_GOUT>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
-																		   g, gstride, pl_lo, pl_hi);
+			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_GOUT, false, false>(
+				buf, pstride, 0, false, base0, 1u, tab, nullptr, 0, g, gstride, pl_lo, pl_hi);
 		else
 		{
-			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map>(buf, pstride, 0, false, base0, 1u, tab, nullptr, 0,
-																  nullptr, 0, pl_lo, pl_hi);
+			pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_SMEM, false, false>(
+				buf, pstride, 0, false, base0, 1u, tab, nullptr, 0, nullptr, 0, pl_lo, pl_hi);
 			__syncthreads();
 		}
 	});
@@ -959,7 +965,7 @@ __device__ __forceinline__ void row_body(const Args &a, const TestDesc &d, uint3
 	const int k = static_cast<int>(blockIdx.x) / P, pl = static_cast<int>(blockIdx.x) % P;
 	if (pl >= W) return;
 	uint32_t *buf = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(k) * S::C;
-	const uint32_t base = (1u << lr) + static_cast<uint32_t>(k);
+	const uint32_t base = a.twist ? 1u : (1u << lr) + static_cast<uint32_t>(k);
 	using MP = RowMap<LC>;
 
 	if (a.op != OP_FWD)
@@ -1089,7 +1095,7 @@ __global__ void __launch_bounds__(row_threads(LC), row2_min_blocks(LC)) k_row2(c
 	const size_t N = size_t(1) << n;
 	const int k = static_cast<int>(blockIdx.x) >> 2, pl = static_cast<int>(blockIdx.x) & 3;
 	const size_t off = static_cast<size_t>(pl) * N + static_cast<size_t>(k) * S::C;
-	row_core_pair<2, LC, RowMap<LC>>(sm, sm + S::PC, (1u << lr) + static_cast<uint32_t>(k), a.tab[2],
+	row_core_pair<2, LC, RowMap<LC>>(sm, sm + S::PC, a.twist ? 1u : (1u << lr) + static_cast<uint32_t>(k), a.tab[2],
 									 d0.zp + off, d1.zp + off, a.op, d0.planes + off, d1.planes + off, pl, store1);
 }
 
@@ -1187,6 +1193,64 @@ __device__ __forceinline__ void inv_thread(const Z &z, uint32_t (&x)[1 << L], ui
 // R1 + m.  Tile: R2 rows x CW columns of every plane, planes in and out.
 constexpr int MID_LR1 = 4;
 
+// The six-step twist.  Row k of the R x C matrix the middle pass leaves
+// (R = 2^lr, element c of row k at k C + c) is the block of the negacyclic
+// transform at table base R + k.  Its evaluation points are nu_k times those
+// of the length-C transform at base 1, nu_k = psi^(2 brev_lr(k) + 1 - R), so
+// its forward transform is the base-1 transform of the row with element c
+// multiplied by nu_k^c, and its inverse is the base-1 inverse followed by
+// nu_k^-c.  With the twist in the middle pass every row reads the same C - 1
+// roots (entries 1 .. C-1 of the table, psi^(R brev(e)) = the roots of the
+// length-C transform) instead of its own.  With k = m 2^LR2 + q (m the
+// middle block, q the register):
+//     nu_k^c = H[m][c] G[c]^brev_LR2(q),
+//     H[m][c] = psi^(c (2 brev_4(m) + 1 - R)),  G[c] = psi^(32 c).
+// Table of one prime and direction (k_twist; psi^-1 for the inverse): H as
+// 16 C words in Montgomery form, then G as C root entries.  (The 64-row
+// pair pass, k_midp, does not twist: at its register limit the twist cost
+// more than the rows gained.)
+__host__ __device__ constexpr int brev_c(int j, int bits)
+{
+	int r = 0;
+	for (int i = 0; i < bits; ++i) r |= ((j >> i) & 1) << (bits - 1 - i);
+	return r;
+}
+
+__device__ __forceinline__ void load_root(RootS &r, const uint32_t *t, size_t i)
+{
+	const uint2 u = __ldg(reinterpret_cast<const uint2 *>(t) + i);
+	r = RootS{ u.x, u.y };
+}
+
+__device__ __forceinline__ void load_root(RootM &r, const uint32_t *t, size_t i) { r = RootM{ __ldg(t + i) }; }
+
+// x[i] times f g^brev_LB(i) for i < 2^LB (f in Montgomery form, g a root entry).
+template <class Z, int LB>
+__device__ __forceinline__ void twist_regs(const Z &z, uint32_t (&x)[1 << LB], uint32_t f, typename Z::root_t g)
+{
+#pragma unroll
+	for (int j = 0; j < (1 << LB); ++j)
+	{
+		const int i = brev_c(j, LB);
+		x[i] = z.mul(x[i], f);
+		if (j + 1 < (1 << LB)) f = z.mulr(f, g);
+	}
+}
+
+// H[m][c] and G[c] of a twist table with C columns.
+__device__ __forceinline__ uint32_t twist_start(const uint32_t *tt, int m, size_t c, size_t C)
+{
+	return __ldg(tt + static_cast<size_t>(m) * C + c);
+}
+
+template <class Z>
+__device__ __forceinline__ typename Z::root_t twist_step(const uint32_t *tt, size_t c, size_t C)
+{
+	typename Z::root_t g;
+	load_root(g, tt + 16 * C, c);
+	return g;
+}
+
 // Unpadded column tile of the middle pass (no CRT reads it): a warp's 32
 // consecutive columns of one row are 32 consecutive words, and the 16-byte
 // staging writes of 8 consecutive threads cover whole rows.
@@ -1276,12 +1340,29 @@ __device__ __forceinline__ void midr_body(const Args &a, const TestDesc &d, int 
 	uint32_t *p = ((a.op == OP_FWD) ? d.zp : d.planes) + static_cast<size_t>(pl) * N +
 				  ((static_cast<size_t>(m) << LR2) << lc) + c;
 	const auto z = prime_rt<SET>(pl);
+	using Z = decltype(z);
 	uint32_t x[1 << LR2];
 #pragma unroll
 	for (int k = 0; k < (1 << LR2); ++k) x[k] = p[k * C];
 	const uint32_t base = (1u << MID_LR1) + static_cast<uint32_t>(m);
-	if constexpr (INV) inv_thread<decltype(z), LR2>(z, x, base, a.tab[SET].iv[pl]);
-	else fwd_thread<decltype(z), LR2>(z, x, base, a.tab[SET].fw[pl]);
+	if constexpr (INV)
+	{
+		if (a.twist)
+		{
+			const uint32_t *tt = a.tab[SET].ti[pl];
+			twist_regs<Z, LR2>(z, x, twist_start(tt, m, c, C), twist_step<Z>(tt, c, C));
+		}
+		inv_thread<Z, LR2>(z, x, base, a.tab[SET].iv[pl]);
+	}
+	else
+	{
+		fwd_thread<Z, LR2>(z, x, base, a.tab[SET].fw[pl]);
+		if (a.twist)
+		{
+			const uint32_t *tt = a.tab[SET].tf[pl];
+			twist_regs<Z, LR2>(z, x, twist_start(tt, m, c, C), twist_step<Z>(tt, c, C));
+		}
+	}
 #pragma unroll
 	for (int k = 0; k < (1 << LR2); ++k) p[k * C] = x[k];
 }
@@ -2161,6 +2242,40 @@ __global__ void k_roots(uint32_t *fw, uint32_t *iv, uint32_t p, uint32_t psi, ui
 		}
 		w = mulmod_u64(w, psi, p);
 		wi = mulmod_u64(wi, psi_inv, p);
+	}
+}
+
+__device__ __forceinline__ uint32_t powmod_d(uint32_t a, uint64_t e, uint32_t p)
+{
+	uint32_t r = 1;
+	for (; e != 0; e >>= 1)
+	{
+		if (e & 1) r = mulmod_u64(r, a, p);
+		a = mulmod_u64(a, a, p);
+	}
+	return r;
+}
+
+// Twist tables of one prime for a six-step split of 2^n points into R = 2^lr
+// rows (twist_regs): thread i < 16 C writes H[m][c] (i = m C + c) of both
+// directions, threads m = 0 also G[c].  words: root entry size.
+__global__ void k_twist(uint32_t *tf, uint32_t *ti, uint32_t p, uint32_t psi, uint32_t psi_inv, int n, int lr, int words)
+{
+	const uint32_t C = 1u << (n - lr);
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= 16 * C) return;
+	const uint32_t m = i / C, c = i % C;
+	const uint64_t two_n = uint64_t(2) << n;
+	const uint64_t bm = __brev(m) >> 28;
+	const uint64_t e = (uint64_t(c) * (2 * bm + 1) + two_n - ((uint64_t(c) << lr) % two_n)) % two_n;
+	const uint32_t r1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
+	tf[i] = mulmod_u64(powmod_d(psi, e, p), r1, p);
+	ti[i] = mulmod_u64(powmod_d(psi_inv, e, p), r1, p);
+	if (m == 0)
+	{
+		const uint64_t g = (32ull * c) % two_n;
+		put_root_d(tf + 16 * C, c, powmod_d(psi, g, p), p, words);
+		put_root_d(ti + 16 * C, c, powmod_d(psi_inv, g, p), p, words);
 	}
 }
 

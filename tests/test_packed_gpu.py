@@ -56,9 +56,11 @@ def test_packed_vs_oracle(oracle, n, plan, b):
 
 
 @pytest.mark.parametrize("n,plan,b", [(17, 303, 150_000_000), (18, 304, 100_000_002), (20, 305, 50_000_000),
-                                      (21, 307, 77_000_000), (22, 305, 35_000_000), (23, 306, 25_000_002)])
+                                      (21, 307, 77_000_000), (22, 305, 35_000_000), (23, 306, 25_000_002),
+                                      (21, 303, 44_000_002), (21, 304, 40_000_000)])
 def test_packed_six_step_vs_oracle(oracle, n, plan, b):
-    """Packed digits with the six-step split of the half-length transform."""
+    """Packed digits with the six-step split of the half-length transform (from
+    n = 21 the 2^3..2^5-row middle passes twist the rows)."""
     rng = np.random.default_rng(n + 7)
     t = Transform(b, n)
     t.batch.set_plan(plan)

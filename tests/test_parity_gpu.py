@@ -78,6 +78,15 @@ def test_six_step_plan(oracle, n, plan, b):
     check_ops(oracle, b, n, plan=plan, seed=200 + n + plan, steps=3)
 
 
+# Six-step plans whose middle pass twists the rows (the row-pass root tables of one direction
+# reach 32 MB: 8 B per point on the two-prime set, 24 B on the three-prime set), with 2^4 and
+# 2^5-row middle passes; the two-prime base at n = 21 keeps the plain rows.
+@pytest.mark.parametrize("n,plan", [(21, 104), (22, 105)])
+@pytest.mark.parametrize("b", [SMALL_B // 4, LARGE_B])
+def test_twisted_six_step_plans(oracle, n, plan, b):
+    check_ops(oracle, b, n, plan=plan, seed=400 + n + plan, steps=3)
+
+
 # The default unpacked plans of the two largest sizes (106 at n = 22, 107 at n = 23), which
 # serve every base outside the packed-digit range (b < 2^20, or above the packed limit):
 # squarings, dup squarings, mul by a register and initMultiplicand + mul against the oracle.
