@@ -47,6 +47,7 @@ struct TestDesc
 	uint32_t *zp;           // 3 x N multiplicand (transform domain, normal form)
 	int64_t *carry;         // N / SEG segment carries
 	const uint32_t *ebits;  // exponent bits, bit i in word i/32 (may be null)
+	uint64_t ewords;        // words ebits holds (0 with ebits null)
 	CarryK ck;              // constants of the fused CRT + carry for this b
 	PackK pk;               // packed-digit constants (set 2)
 	uint32_t b;
@@ -78,6 +79,7 @@ struct Args
 	int fix;                // four-step column-forward: register src has pending segment carries
 	int pdl_graph;          // host only: graph-captured launches keep programmatic edges
 	int twist;              // six-step: the middle pass twists, every row transform has base 1
+	uint32_t ntests;        // tests of the batch (0: unchecked); the guard of test_ok
 };
 
 template <int SET, int PL>
@@ -99,6 +101,37 @@ __device__ __forceinline__ bool exp_bit(const uint32_t *ebits, int64_t i)
 	return ((__ldg(&ebits[i >> 5]) >> (i & 31)) & 1u) != 0;
 }
 
+// Error word bits: 1 a segment carry not absorbed, 2 a guard (below) tripped.
+constexpr uint32_t ERR_CARRY = 1u, ERR_GUARD = 2u;
+
+// The guard of every kernel that takes a test from the launch's list: the
+// test index lies in the batch (with dup_bit below, the exponent position in
+// the test's exponent words).  A corrupted list would otherwise make the
+// kernel touch memory it does not own; instead the guard records ERR_GUARD
+// (reported by the next synchronising call) and the test is skipped.  Checked
+// when the launch carries the batch's size (a.ntests != 0).  Measured on one
+// B200: 0.4 % of a 64-test n = 16 squaring (89.8 -> 90.2 us); checking every
+// descriptor pointer against the batch's allocation as well (four more loads
+// per CTA) cost 2.9 %.
+__device__ __forceinline__ bool test_ok(const Args &a, int t)
+{
+	const bool ok = (a.ntests == 0) || (static_cast<uint32_t>(t) < a.ntests);
+	if (!ok) atomicOr(a.err, ERR_GUARD);
+	return ok;
+}
+
+// Exponent bit i of test d, guarded: a position beyond the test's exponent
+// words records ERR_GUARD and reads as 0.
+__device__ __forceinline__ bool dup_bit(const Args &a, const TestDesc &d, int64_t i)
+{
+	if ((d.ebits == nullptr) || (static_cast<uint64_t>(i >> 5) >= d.ewords))
+	{
+		atomicOr(a.err, ERR_GUARD);
+		return false;
+	}
+	return exp_bit(d.ebits, i);
+}
+
 // Programmatic dependent launch: a kernel launched with programmatic stream
 // serialization may be scheduled while the previous kernel of its stream is
 // still running; it waits here (griddepcontrol.wait returns once every
@@ -115,12 +148,13 @@ __device__ __forceinline__ void pdl_wait()
 // `active` cleared when the test has no squaring left.
 __device__ __forceinline__ bool get_dup(const Args &a, const TestDesc &d, int t, int j, bool &active)
 {
-	active = true;
+	active = test_ok(a, t);
+	if (!active) return false;
 	if (a.dup_mode == DUP_BITS)
 	{
 		const int64_t i = a.pos[t] - j;
 		if (i < 0) { active = false; return false; }
-		return exp_bit(d.ebits, i);
+		return dup_bit(a, d, i);
 	}
 	return a.dup_mode == DUP_ALL;
 }
@@ -606,6 +640,7 @@ __global__ void __launch_bounds__(SmallShape<SET, LOGN, SPLIT>::T, SmallShape<SE
 	pdl_wait();
 	extern __shared__ __align__(16) uint32_t sm[];
 	const int t = a.tests[blockIdx.x];
+	if (!test_ok(a, t)) return;
 	small_body<SET, LOGN, SPLIT>(a, t, a.desc[t], sm);
 }
 
@@ -761,7 +796,7 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 
 	for (int it = 0; it < iters; ++it)
 	{
-		const bool dup = (a.dup_mode == DUP_BITS) ? exp_bit(d.ebits, pos0 - it) : (a.dup_mode == DUP_ALL);
+		const bool dup = (a.dup_mode == DUP_BITS) ? dup_bit(a, d, pos0 - it) : (a.dup_mode == DUP_ALL);
 		if (owner)
 		{
 			for_planes<SET>([&](auto PLc) {
@@ -833,8 +868,11 @@ __global__ void __launch_bounds__(ClusterShape<LQ, LC>::T, ClusterShape<LQ, LC>:
 	for (int ti = cid; ti < ntests; ti += ncl)
 	{
 		const int t = a.tests[ti];
-		const TestDesc &d = a.desc[t];
-		if (d.set == 0) cluster_test<0, LQ, LC>(a, t, d, sm, q); else cluster_test<1, LQ, LC>(a, t, d, sm, q);
+		if (test_ok(a, t))
+		{
+			const TestDesc &d = a.desc[t];
+			if (d.set == 0) cluster_test<0, LQ, LC>(a, t, d, sm, q); else cluster_test<1, LQ, LC>(a, t, d, sm, q);
+		}
 		// the next test's first shared-memory writes follow this barrier, after
 		// every CTA has read this test's last carries
 		cl.sync();
@@ -1869,15 +1907,22 @@ __device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, 
 	{
 		const int k = e / SPR, s = e % SPR;
 		const size_t i0 = static_cast<size_t>(k) * Cp + c0 + static_cast<size_t>(s) * (SEG / 2);
+		// Garner's digits of the segment's eight coefficients first (independent
+		// of one another), then the digit window's dependent chain
 		int64_t win[7] = { 0, 0, 0, 0, 0, 0, 0 };
 		int32_t dg[SEG];
+		uint32_t g[SEG / 2][4];
 #pragma unroll
 		for (int ci = 0; ci < SEG / 2; ++ci)
 		{
-			uint32_t x[4];
 #pragma unroll
-			for (int pl = 0; pl < 4; ++pl) x[pl] = sm[pl * PS + S::addr(k, s * (SEG / 2) + ci)];
-			crt_window(x, dup ? 1 : 0, d.pk, win);
+			for (int pl = 0; pl < 4; ++pl) g[ci][pl] = sm[pl * PS + S::addr(k, s * (SEG / 2) + ci)];
+			crt_garner4(g[ci]);
+		}
+#pragma unroll
+		for (int ci = 0; ci < SEG / 2; ++ci)
+		{
+			crt_window_g(g[ci], dup ? 1 : 0, d.pk, win);
 			dg[2 * ci] = window_digit(d.ck, win);
 			dg[2 * ci + 1] = window_digit(d.ck, win);
 		}
@@ -2143,6 +2188,7 @@ __global__ void __launch_bounds__(256) k_mulscalar(const Args a, int32_t m)
 {
 	pdl_wait();
 	const int t = a.tests[blockIdx.y];
+	if (!test_ok(a, t)) return;
 	const TestDesc &d = a.desc[t];
 	const size_t N = size_t(1) << a.n;
 	const size_t s = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -2170,6 +2216,7 @@ __global__ void k_set(const Args a, int32_t value)
 {
 	pdl_wait();
 	const int t = a.tests[blockIdx.y];
+	if (!test_ok(a, t)) return;
 	const size_t N = size_t(1) << a.n;
 	int32_t *r = a.desc[t].regs + static_cast<size_t>(a.dst) * N;
 	for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x)
@@ -2181,6 +2228,7 @@ __global__ void k_copy(const Args a)
 {
 	pdl_wait();
 	const int t = a.tests[blockIdx.y];
+	if (!test_ok(a, t)) return;
 	const size_t N = size_t(1) << a.n;
 	const int4 *s = reinterpret_cast<const int4 *>(a.desc[t].regs + static_cast<size_t>(a.src) * N);
 	int4 *o = reinterpret_cast<int4 *>(a.desc[t].regs + static_cast<size_t>(a.dst) * N);
@@ -2285,7 +2333,7 @@ __global__ void k_pos_sub(int64_t *pos, const int32_t *tests, int ntests, int co
 {
 	pdl_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < ntests)
+	if ((i < ntests) && (static_cast<uint32_t>(tests[i]) < static_cast<uint32_t>(ntests)))
 	{
 		const int64_t p = pos[tests[i]] - count;
 		pos[tests[i]] = (p < -1) ? -1 : p;

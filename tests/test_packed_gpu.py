@@ -128,6 +128,26 @@ def test_packed_graph_blocks_match_unpacked(n, plan):
         assert np.array_equal(canon(got[2][i], b), canon(ref[2][i], b)), i
 
 
+@pytest.mark.parametrize("n,plan,ref,count", [(21, 303, 8, 5), (21, 304, 8, 5), (21, 305, 8, 4), (22, 304, 9, 3),
+                                              (22, 305, 9, 3)])
+def test_twisted_packed_blocks_match_four_step(n, plan, ref, count):
+    """Batches on twisted six-step packed plans (two tests per row CTA, every
+    row at table base 1) against the unpacked four-step plan, which has no
+    middle pass: Gerbicz-Li blocks with exponents of different lengths, so that
+    tests drop out at different squarings of the last block and row CTAs run
+    pairs with one test left (and, with an odd count, a lone last test)."""
+    rng = np.random.default_rng(n + plan)
+    bases = [int(x) & ~1 for x in rng.integers(1_100_000, 30_000_000, size=count)]
+    B = 20
+    exps = [gf.Job.prefix(b, n, 4 * B + (i % 5)).words_nbits() for i, b in enumerate(bases)]
+    got = _blocks(bases, n, plan, B, 2, exps)
+    want = _blocks(bases, n, ref, B, 2, exps)
+    assert np.array_equal(got[0], want[0])
+    for i, b in enumerate(bases):
+        assert np.array_equal(canon(got[1][i], b), canon(want[1][i], b)), i
+        assert np.array_equal(canon(got[2][i], b), canon(want[2][i], b)), i
+
+
 def test_plan_switch_with_pending_carries(oracle):
     """Carries left pending by one plan are absorbed before the next takes over."""
     n, b = 16, 60_000_002

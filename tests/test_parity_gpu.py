@@ -255,3 +255,29 @@ def test_square_mul(oracle, b, plan):
         g = t.getInt()
         assert np.abs(g).max() <= b // 2 + 1
         assert np.array_equal(canon(g, b), canon(o.getInt(), b)), f"a={a}"
+
+
+@pytest.mark.parametrize("b", [10, 1026, LARGE_B])
+def test_digit_range_checked_on_load(b):
+    """gfc_batch_set_zi / gfc_batch_set_all accept |d| <= b/2 + 1 and refuse one
+    digit beyond it (either sign, any position) with GFC_ERR_ARG, leaving the
+    register as it was."""
+    from genefer22_b200._lib import GfcError
+    n, lim = 12, b // 2 + 1
+    rng = np.random.default_rng(b)
+    with Batch([b, b], n) as bt:
+        ok = rand_digits(rng, b, 1 << n)
+        ok[0], ok[-1], ok[7] = lim, -lim, lim
+        bt.put(0, ok)
+        assert np.array_equal(bt.get(0), ok)
+        for pos, v in ((5, lim + 1), ((1 << n) - 1, -lim - 1), (0, 2**31 - 1), (3, -2**31)):
+            bad = ok.copy()
+            bad[pos] = v
+            with pytest.raises(GfcError):
+                bt.put(0, bad)
+            both = np.stack([ok, bad])
+            with pytest.raises(GfcError):
+                bt.put_all(both)
+            assert np.array_equal(bt.get(0), ok)
+        bt.put_all(np.stack([ok, ok]))
+        assert np.array_equal(bt.get_all(0)[1], ok)
