@@ -647,7 +647,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="batch", choices=["batch", "uneven", "serve", "sizes", "verify"],
                     help="batch: the default line; the others print their own line")
-    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=40)
     ap.add_argument("--no-extras", action="store_true", help="skip the north-star block of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
