@@ -621,7 +621,14 @@ void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 {
 	using S = RowShape<LC>;
 	const size_t smem = size_t(S::PC) * 4;          // one plane per CTA
-	if (prep) { set_smem(k_row<LC>, smem); set_smem(k_row2<LC>, 2 * smem); return; }
+	if (prep) { set_smem(k_row<LC>, smem); set_smem(k_row2<LC>, 2 * smem); set_smem(k_rowp<LC>, 2 * smem); return; }
+	if ((planes == 4) && (a.op != OP_FWD) && a.twist)
+	{
+		// twisted packed rows share their roots: two rows of a test per CTA (k_rowp)
+		const dim3 grid((1u << (a.n - LC - 1)) * 4u, static_cast<unsigned>(grid_y));
+		launch_pdl(k_rowp<LC>, grid, dim3(row_threads(LC)), 2 * smem, s, a);
+		return;
+	}
 	if ((planes == 4) && (a.op != OP_FWD) && (grid_y >= 2))
 	{
 		// packed batches: two tests per CTA sharing the row's roots (k_row2)

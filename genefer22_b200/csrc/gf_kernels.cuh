@@ -1137,6 +1137,29 @@ __global__ void __launch_bounds__(row_threads(LC), row2_min_blocks(LC)) k_row2(c
 									 d0.zp + off, d1.zp + off, a.op, d0.planes + off, d1.planes + off, pl, store1);
 }
 
+// Rows of a twisted packed launch, two rows of one test per CTA: with the
+// six-step twist every row transforms with the roots of base 1, so the pair
+// shares each group's roots and runs two independent butterfly chains, as
+// k_row2 does for two tests.  blockIdx.x = row pair * 4 + plane, blockIdx.y =
+// the launch's test.  Squarings and products only.
+template <int LC>
+__global__ void __launch_bounds__(row_threads(LC), row2_min_blocks(LC)) k_rowp(const Args a)
+{
+	pdl_wait();
+	extern __shared__ __align__(16) uint32_t sm[];
+	using S = RowShape<LC>;
+	const int t = a.tests[blockIdx.y];
+	const TestDesc &d = a.desc[t];
+	bool active;
+	(void)get_dup(a, d, t, a.j, active);
+	if (!active) return;
+	const size_t N = size_t(1) << a.n;
+	const int k = 2 * (static_cast<int>(blockIdx.x) >> 2), pl = static_cast<int>(blockIdx.x) & 3;
+	const size_t off = static_cast<size_t>(pl) * N + static_cast<size_t>(k) * S::C;
+	row_core_pair<2, LC, RowMap<LC>>(sm, sm + S::PC, 1u, a.tab[2], d.zp + off, d.zp + off + S::C, a.op,
+									 d.planes + off, d.planes + off + S::C, pl, true);
+}
+
 // Columns: last log2 R inverse stages, CRT, carry inside 16-digit segments.
 template <int LR>
 __global__ void __launch_bounds__(col_threads(LR)) k_col_inv(const Args a)
