@@ -677,8 +677,19 @@ void pcol_t(bool inv, const Args &a, int grid_y, cudaStream_t s, bool prep)
 	if (split_cols(cols, grid_y, 32))
 	{
 		const dim3 grid(static_cast<unsigned>(cols / PCS_T), static_cast<unsigned>(grid_y));
-		if (inv) launch_pdl(k_pcol_inv_s<LR>, grid, dim3(4 * PCS_T), 0, s, a);
-		else launch_pdl(k_pcol_fwd_s<LR>, grid, dim3(4 * PCS_T), 0, s, a);
+		// from 1024 CTAs (more than a wave at six CTAs per SM) six CTAs per SM
+		// at 40 registers, else four at 64: one packed test per squaring, graph
+		// replay on one B200, n = 22 135.8 -> 131.9 us, n = 21 73.6 -> 72.7,
+		// four tests at n = 19 64.9 -> 64.2; a smaller grid (one test at n = 20,
+		// 512 CTAs) ran 43.2 -> 47.5 us with the 40-register form
+		const bool hi = size_t(grid.x) * grid.y >= 1024;
+		if (inv)
+		{
+			if (hi) launch_pdl(k_pcol_inv_s<LR, PCS_MINB_HI>, grid, dim3(4 * PCS_T), 0, s, a);
+			else launch_pdl(k_pcol_inv_s<LR, PCS_MINB_LO>, grid, dim3(4 * PCS_T), 0, s, a);
+		}
+		else if (hi) launch_pdl(k_pcol_fwd_s<LR, PCS_MINB_HI>, grid, dim3(4 * PCS_T), 0, s, a);
+		else launch_pdl(k_pcol_fwd_s<LR, PCS_MINB_LO>, grid, dim3(4 * PCS_T), 0, s, a);
 		return;
 	}
 	const dim3 grid(static_cast<unsigned>(cols / PCOL_THREADS), static_cast<unsigned>(grid_y));

@@ -2117,8 +2117,13 @@ __device__ __forceinline__ void pcol_inv_split_body(const Args &a, const TestDes
 	}
 }
 
-template <int LR>
-__global__ void __launch_bounds__(4 * PCS_T) k_pcol_fwd_s(const Args a)
+// MINB = PCS_MINB_HI caps the registers at 40 for six CTAs per SM, the form
+// for large launches; PCS_MINB_LO at 64 for four (with no minimum ptxas
+// gave the inverse kernel 80 registers, three CTAs per SM).
+constexpr int PCS_MINB_HI = 6, PCS_MINB_LO = 4;
+
+template <int LR, int MINB>
+__global__ void __launch_bounds__(4 * PCS_T, MINB) k_pcol_fwd_s(const Args a)
 {
 	pdl_wait();
 	__shared__ int32_t sm[(1 << LR) * (2 * PCS_T + 2 * PCS_T / SEG)];
@@ -2130,8 +2135,8 @@ __global__ void __launch_bounds__(4 * PCS_T) k_pcol_fwd_s(const Args a)
 	pcol_fwd_split_body<LR>(a, d, sm);
 }
 
-template <int LR>
-__global__ void __launch_bounds__(4 * PCS_T) k_pcol_inv_s(const Args a)
+template <int LR, int MINB>
+__global__ void __launch_bounds__(4 * PCS_T, MINB) k_pcol_inv_s(const Args a)
 {
 	pdl_wait();
 	__shared__ __align__(16) uint32_t sm[4 * PColShapeS<LR>::PS];
