@@ -1111,7 +1111,10 @@ __global__ void __launch_bounds__(row_threads(LC)) k_row(const Args a)
 // products only (the forward transform of a multiplicand runs k_row).  A pair
 // with one test left (the other one past its exponent, or an odd count) runs
 // that test on both lanes and writes it once.
-__host__ __device__ constexpr int row2_min_blocks(int lc) { return (row_threads(lc) >= 512) ? 1 : 3; }
+// Four CTAs per SM at 64 registers (16 bytes spilled) for rows of at most
+// 4096 points: with the 8-row columns at five, the n = 16 batch 90.1 -> 89.0 us
+// per squaring, 16 tests at n = 17 57.5 -> 57.0, against three at 80.
+__host__ __device__ constexpr int row2_min_blocks(int lc) { return (row_threads(lc) >= 512) ? 1 : 4; }
 
 template <int LC>
 __global__ void __launch_bounds__(row_threads(LC), row2_min_blocks(LC)) k_row2(const Args a, int ntests)
@@ -1960,7 +1963,10 @@ __device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, 
 
 // 16-row columns hold 32 digits and 15 two-word roots per thread: three CTAs
 // per SM leave them 85 registers (the inverse kernel's tile fits three anyway).
-__host__ __device__ constexpr int pcol_min_blocks(int lr) { return (lr >= 4) ? 3 : 4; }
+// 8-row columns at five CTAs per SM (48 registers; 16 bytes spilled in the
+// forward kernel): the 64-test n = 16 batch 90.1 -> 89.3 us per squaring
+// against four, 93.7 at six (40 registers, 60 bytes spilled).
+__host__ __device__ constexpr int pcol_min_blocks(int lr) { return (lr >= 4) ? 3 : 5; }
 
 template <int LR>
 __global__ void __launch_bounds__(PCOL_THREADS, pcol_min_blocks(LR)) k_pcol_fwd(const Args a)
