@@ -2257,6 +2257,40 @@ __global__ void k_set(const Args a, int32_t value)
 		r[i] = (i == 0) ? value : 0;
 }
 
+// Digits loaded into a test's planes (its transform scratch, N words at
+// d.planes) checked against |d| <= b/2 + 1: any digit outside sets *bad.
+// blockIdx.y = test, four digits per thread.
+__global__ void __launch_bounds__(256) k_check_digits(const TestDesc *desc, int n, uint32_t *bad)
+{
+	const TestDesc &d = desc[blockIdx.y];
+	const size_t N = size_t(1) << n;
+	const uint32_t lim = d.b / 2 + 1, span = 2 * lim;
+	const int4 *src = reinterpret_cast<const int4 *>(d.planes);
+	uint32_t out = 0;
+	for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N / 4; i += size_t(gridDim.x) * blockDim.x)
+	{
+		const int4 v = src[i];
+		out |= static_cast<uint32_t>(static_cast<uint32_t>(v.x) + lim > span) |
+			   static_cast<uint32_t>(static_cast<uint32_t>(v.y) + lim > span) |
+			   static_cast<uint32_t>(static_cast<uint32_t>(v.z) + lim > span) |
+			   static_cast<uint32_t>(static_cast<uint32_t>(v.w) + lim > span);
+	}
+	if (__any_sync(0xffffffffu, out != 0) && ((threadIdx.x & 31) == 0)) atomicOr(bad, 1u);
+}
+
+// Register reg of every test <- the digits staged in its planes, unless *bad
+// (then every register stays as it was).
+__global__ void __launch_bounds__(256) k_commit_digits(const TestDesc *desc, int n, int reg, const uint32_t *bad)
+{
+	if (*bad != 0) return;
+	const TestDesc &d = desc[blockIdx.y];
+	const size_t N = size_t(1) << n;
+	const int4 *src = reinterpret_cast<const int4 *>(d.planes);
+	int4 *dst = reinterpret_cast<int4 *>(d.regs + static_cast<size_t>(reg) * N);
+	for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N / 4; i += size_t(gridDim.x) * blockDim.x)
+		dst[i] = src[i];
+}
+
 // reg[dst] = reg[src] for every test of the launch.
 __global__ void k_copy(const Args a)
 {
