@@ -124,6 +124,16 @@ struct Zp
 		return (hi < mh) ? u + P : u;
 	}
 
+	// t 2^-32 mod p for t < p 2^32 (Montgomery reduction; result in [0, p)).
+	__device__ __forceinline__ static uint32_t redc64(uint64_t t)
+	{
+		const uint32_t lo = static_cast<uint32_t>(t), hi = static_cast<uint32_t>(t >> 32);
+		const uint32_t mh = __umulhi(lo * q, P);
+		const uint32_t u = hi - mh;
+		if (P31) return min(u, u + P);
+		return (hi < mh) ? u + P : u;
+	}
+
 	// signed digit -> residue (|d| < p)
 	__device__ __forceinline__ static uint32_t from_int(int32_t d)
 	{
@@ -160,6 +170,15 @@ struct ZpR
 	__device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const
 	{
 		const uint64_t t = static_cast<uint64_t>(a) * b;
+		const uint32_t lo = static_cast<uint32_t>(t), hi = static_cast<uint32_t>(t >> 32);
+		const uint32_t mh = __umulhi(lo * q, p);
+		const uint32_t u = hi - mh;
+		if (P31) return min(u, u + p);
+		return (hi < mh) ? u + p : u;
+	}
+
+	__device__ __forceinline__ uint32_t redc64(uint64_t t) const
+	{
 		const uint32_t lo = static_cast<uint32_t>(t), hi = static_cast<uint32_t>(t >> 32);
 		const uint32_t mh = __umulhi(lo * q, p);
 		const uint32_t u = hi - mh;
@@ -346,8 +365,26 @@ struct PackK
 	uint32_t w1[2][2];          // limbs 0..1 of f p1
 	uint32_t w2[2][4];          // limbs 0..3 of f p1 p2
 	uint32_t w3[2][5];          // limbs 0..4 of f p1 p2 p3
-	uint32_t bm[4];             // b mod p_k in Montgomery form (packing d0 + b d1)
+	uint32_t bm[4];             // b mod p_k in Montgomery form (packing d0 + b d1 in 16-row columns)
 };
+
+// A packed coefficient D = d0 + b d1 of two resting digits (|d| <= b/2 + 1,
+// b < 2^28: |D| < 2^55) as the residue D 2^-32 mod p of a set-2 prime: one
+// Montgomery reduction of D + 2^25 p, which lies in (0, p 2^32) since
+// p > 2^30.  The 8-row packed column kernels pack this way; the factor 2^-32
+// on their inputs is compensated by the normalisation in word 1 of entry 0
+// of the set-2 root tables (word 0 holds the one for D itself, which the
+// 16-row column kernels make as d0 + (b mod p) d1).
+__device__ __forceinline__ int64_t pack_value(int32_t d0, int32_t d1, uint32_t b)
+{
+	return static_cast<int64_t>(d0) + static_cast<int64_t>(static_cast<int32_t>(b)) * static_cast<int64_t>(d1);
+}
+
+template <class Z>
+__device__ __forceinline__ uint32_t pack_residue(const Z &z, int64_t D)
+{
+	return z.redc64(static_cast<uint64_t>(D + (static_cast<int64_t>(z.p) << 25)));
+}
 
 // Garner's mixed-radix digits a1..a4 of one packed coefficient (residues
 // x[4]), a4 carrying in bit 31 the flag V > M/2 (a4 < p4 < 2^31).

@@ -136,7 +136,7 @@ inline void put_root(uint32_t *t, size_t k, uint32_t w, uint32_t p)
 // The host finds psi and the entry-0 constants; the kernel writes the N
 // entries of both tables with one product per entry.  fw and iv are device
 // pointers; `s` a stream of the device.
-void build_roots_device(uint32_t p, int n, uint32_t *fw, uint32_t *iv, cudaStream_t s)
+void build_roots_device(uint32_t p, int n, uint32_t *fw, uint32_t *iv, cudaStream_t s, bool packed = false)
 {
 	const uint32_t N = 1u << n;
 	const uint32_t psi = powmod_h(primitive_root(p), (p - 1) / (2ull * N), p);
@@ -145,10 +145,14 @@ void build_roots_device(uint32_t p, int n, uint32_t *fw, uint32_t *iv, cudaStrea
 	const uint32_t R1 = static_cast<uint32_t>((uint64_t(1) << 32) % p);
 	const uint32_t c = mulmod_h(mulmod_h(R1, R1, p), powmod_h(N % p, p - 2, p), p);
 	const uint32_t k0 = mulmod_h(p - powmod_h(psi, N / 2, p), c, p);
+	// word 1 of entry 0 (31-bit primes): for inputs packed as D 2^-32
+	// (pack_residue, the packed tables' 8-row columns), 2^64 more on the square
+	const uint32_t c2 = packed ? mulmod_h(c, mulmod_h(R1, R1, p), p) : 0u;
+	const uint32_t k02 = packed ? mulmod_h(p - powmod_h(psi, N / 2, p), c2, p) : 0u;
 	const int run = 64, threads = 256;
 	const uint32_t runs = (N + run - 1) / run;
 	k_roots<<<(runs + threads - 1) / threads, threads, 0, s>>>(fw, iv, p, psi, psi_inv, n, static_cast<int>(root_words(p)),
-															   run, c, k0);
+															   run, c, k0, c2, k02);
 	const cudaError_t e = cudaGetLastError();
 	if (e != cudaSuccess) fail(GFC_ERR_CUDA, std::string("root table kernel: ") + cudaGetErrorString(e));
 }
@@ -433,7 +437,7 @@ std::shared_ptr<DeviceTables> get_tables_packed(int device, int np)
 		{
 			t->tab[2].fw[pl] = t->d + (2 * pl) * words;
 			t->tab[2].iv[pl] = t->d + (2 * pl + 1) * words;
-			build_roots_device(PrimeSet<2>::p[pl], np, t->d + (2 * pl) * words, t->d + (2 * pl + 1) * words, ts.s);
+			build_roots_device(PrimeSet<2>::p[pl], np, t->d + (2 * pl) * words, t->d + (2 * pl + 1) * words, ts.s, true);
 		}
 		ts.sync();
 	}

@@ -1809,6 +1809,10 @@ __global__ void __launch_bounds__(WMAX * CS_T) k_colr_inv_s(const Args a)
 
 constexpr int PCOL_THREADS = 256;
 
+// The word of root-table entry 0 that holds the normalisation of a packed
+// column size: 1 (for inputs D 2^-32) with 8-row columns, 0 with 16-row ones.
+__host__ __device__ constexpr int pcol_norm_word(int lr) { return (lr == 3) ? 1 : 0; }
+
 // Takes (and clears) the packed carry into segment s: the previous
 // segment's, negated across the wrap (b^N = -1).
 __device__ __forceinline__ void take_carry5(const TestDesc &d, size_t s, size_t nseg, int64_t (&c)[PK_CARRY],
@@ -1880,13 +1884,23 @@ __device__ __forceinline__ void pcol_fwd_body(const Args &a, const TestDesc &d, 
 #pragma unroll
 		for (int k = 0; k < R; ++k) { d0[k] = sm[k * RW + o]; d1[k] = sm[k * RW + o + 1]; }
 	}
+	// 8-row columns pack as D 2^-32 (pack_residue), 16-row ones as D
+	const uint32_t bb = d.b;
 	for_planes<2>([&](auto PLc) {
 		constexpr int PL = decltype(PLc)::value;
 		using Z = ZS<2, PL>;
-		const uint32_t bm = d.pk.bm[PL];
 		uint32_t x[R];
+		if constexpr (LR == 3)
+		{
 #pragma unroll
-		for (int k = 0; k < R; ++k) x[k] = Z::add(Z::from_int(d0[k]), Z::mul(Z::from_int(d1[k]), bm));
+			for (int k = 0; k < R; ++k) x[k] = pack_residue(Z{}, pack_value(d0[k], d1[k], bb));
+		}
+		else
+		{
+			const uint32_t bm = d.pk.bm[PL];
+#pragma unroll
+			for (int k = 0; k < R; ++k) x[k] = Z::add(Z::from_int(d0[k]), Z::mul(Z::from_int(d1[k]), bm));
+		}
 		fwd_reg<Z, LR>(Z{}, x, 1u, a.tab[2].fw[PL]);
 #pragma unroll
 		for (int k = 0; k < R; ++k) dst[PL * Np + k * Cp] = x[k];
@@ -1923,7 +1937,8 @@ __device__ __forceinline__ void pcol_inv_body(const Args &a, const TestDesc &d, 
 		uint32_t x[R];
 #pragma unroll
 		for (int k = 0; k < R; ++k) x[k] = src[k * Cp];
-		inv_reg<Z, LR>(Z{}, x, 1u, a.tab[2].iv[PL], true, __ldg(&a.tab[2].fw[PL][0]), __ldg(&a.tab[2].iv[PL][0]));
+		inv_reg<Z, LR>(Z{}, x, 1u, a.tab[2].iv[PL], true, __ldg(&a.tab[2].fw[PL][pcol_norm_word(LR)]),
+					   __ldg(&a.tab[2].iv[PL][pcol_norm_word(LR)]));
 #pragma unroll
 		for (int k = 0; k < R; ++k) sm[PL * PS + S::addr(k, tid)] = x[k];
 	});
@@ -2030,7 +2045,7 @@ __device__ __forceinline__ void pcol_fwd_split_body(const Args &a, const TestDes
 		__syncthreads();
 	}
 	const auto z = prime_rt<2>(pl);
-	const uint32_t bm = d.pk.bm[pl];
+	const uint32_t bb = d.b, bm = d.pk.bm[pl];
 	uint32_t x[R];
 #pragma unroll
 	for (int k = 0; k < R; ++k)
@@ -2046,7 +2061,8 @@ __device__ __forceinline__ void pcol_fwd_split_body(const Args &a, const TestDes
 			const int2 v = *reinterpret_cast<const int2 *>(srcreg + 2 * (static_cast<size_t>(k) * Cp + c0 + c));
 			v0 = v.x; v1 = v.y;
 		}
-		x[k] = z.add(z.from_int(v0), z.mul(z.from_int(v1), bm));
+		if constexpr (LR == 3) x[k] = pack_residue(z, pack_value(v0, v1, bb));
+		else x[k] = z.add(z.from_int(v0), z.mul(z.from_int(v1), bm));
 	}
 	fwd_reg<decltype(z), LR>(z, x, 1u, a.tab[2].fw[pl]);
 	uint32_t *dst = ((a.op == OP_FWD) ? d.zp : d.planes) + pl * Np + c0 + c;
@@ -2081,7 +2097,8 @@ __device__ __forceinline__ void pcol_inv_split_body(const Args &a, const TestDes
 		uint32_t x[R];
 #pragma unroll
 		for (int k = 0; k < R; ++k) x[k] = src[k * Cp];
-		inv_reg<decltype(z), LR>(z, x, 1u, a.tab[2].iv[pl], true, __ldg(&a.tab[2].fw[pl][0]), __ldg(&a.tab[2].iv[pl][0]));
+		inv_reg<decltype(z), LR>(z, x, 1u, a.tab[2].iv[pl], true, __ldg(&a.tab[2].fw[pl][pcol_norm_word(LR)]),
+								 __ldg(&a.tab[2].iv[pl][pcol_norm_word(LR)]));
 #pragma unroll
 		for (int k = 0; k < R; ++k) sm[pl * PS + S::addr(k, c)] = x[k];
 	}
@@ -2329,7 +2346,7 @@ __device__ __forceinline__ void put_root_d(uint32_t *t, uint32_t k, uint32_t w, 
 }
 
 __global__ void k_roots(uint32_t *fw, uint32_t *iv, uint32_t p, uint32_t psi, uint32_t psi_inv, int n, int words, int run,
-						uint32_t c, uint32_t k0)
+						uint32_t c, uint32_t k0, uint32_t c2, uint32_t k02)
 {
 	const uint32_t N = 1u << n;
 	const uint32_t e0 = (blockIdx.x * blockDim.x + threadIdx.x) * static_cast<uint32_t>(run);
@@ -2348,7 +2365,7 @@ __global__ void k_roots(uint32_t *fw, uint32_t *iv, uint32_t p, uint32_t psi, ui
 		{
 			fw[0] = c;
 			iv[0] = k0;
-			if (words == 2) { fw[1] = 0; iv[1] = 0; }
+			if (words == 2) { fw[1] = c2; iv[1] = k02; }
 		}
 		else
 		{
