@@ -84,6 +84,12 @@ template <> struct PrimeSet<2>
 struct RootM { uint32_t w; };
 struct RootS { uint32_t w, q; };
 
+// w and floor(w 2^32 / p), at compile time
+__host__ __device__ constexpr RootS shoup_c(uint32_t w, uint32_t p)
+{
+	return RootS{ w, static_cast<uint32_t>((static_cast<uint64_t>(w) << 32) / p) };
+}
+
 // a w mod p for a < 2^32, w < p < 2^31 (Shoup): with h = floor(a q / 2^32),
 // a w - h p lies in [0, 2p), so its low 32 bits are exact.
 __device__ __forceinline__ uint32_t shoup_mul(uint32_t a, RootS r, uint32_t p)
@@ -225,23 +231,26 @@ struct Crt<0>
 template <>
 struct Crt<1>
 {
+	// Garner's constants with their Shoup quotients (the set-1 primes are below 2^31):
+	// p1^-1 mod p2, p1 mod p3, (p1 p2)^-1 mod p3
 	static constexpr uint32_t p1 = PrimeSet<1>::p[0], p2 = PrimeSet<1>::p[1], p3 = PrimeSet<1>::p[2];
-	static constexpr uint32_t c12 = to_mont_c(invmod_c(p1 % p2, p2), p2);                                   // p1^{-1} mod p2
-	static constexpr uint32_t p1m3 = to_mont_c(p1 % p3, p3);                                                 // p1 mod p3
-	static constexpr uint32_t c123 = to_mont_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);   // (p1 p2)^{-1} mod p3
+	static constexpr RootS s12 = shoup_c(invmod_c(p1 % p2, p2), p2);
+	static constexpr RootS s1_3 = shoup_c(p1 % p3, p3);
+	static constexpr RootS s123 = shoup_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);
 };
 
 template <>
 struct Crt<2>
 {
+	// as Crt<1>, and p1 mod p4, p1 p2 mod p4, (p1 p2 p3)^-1 mod p4 (every set-2 prime is below 2^31)
 	static constexpr uint32_t p1 = PrimeSet<2>::p[0], p2 = PrimeSet<2>::p[1], p3 = PrimeSet<2>::p[2], p4 = PrimeSet<2>::p[3];
-	static constexpr uint32_t c12 = to_mont_c(invmod_c(p1 % p2, p2), p2);                                   // p1^{-1} mod p2
-	static constexpr uint32_t p1m3 = to_mont_c(p1 % p3, p3);
-	static constexpr uint32_t c123 = to_mont_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);
-	static constexpr uint32_t p1m4 = to_mont_c(p1 % p4, p4);
-	static constexpr uint32_t p12m4 = to_mont_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p4), p4);
-	static constexpr uint32_t c1234 = to_mont_c(invmod_c(static_cast<uint32_t>(
-		(((static_cast<uint64_t>(p1) * p2) % p4) * p3) % p4), p4), p4);                                 // (p1 p2 p3)^{-1} mod p4
+	static constexpr RootS s12 = shoup_c(invmod_c(p1 % p2, p2), p2);
+	static constexpr RootS s1_3 = shoup_c(p1 % p3, p3);
+	static constexpr RootS s123 = shoup_c(invmod_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p3), p3), p3);
+	static constexpr RootS s1_4 = shoup_c(p1 % p4, p4);
+	static constexpr RootS s12_4 = shoup_c(static_cast<uint32_t>((static_cast<uint64_t>(p1) * p2) % p4), p4);
+	static constexpr RootS s1234 = shoup_c(invmod_c(static_cast<uint32_t>(
+		(((static_cast<uint64_t>(p1) * p2) % p4) * p3) % p4), p4), p4);
 };
 
 // ---------------------------------------------------------------- CRT + base-b carry
@@ -307,9 +316,9 @@ __device__ __forceinline__ int32_t crt_carry<1>(const uint32_t x[3], int dup, co
 	using Z3 = Zp<C::p3, true>;
 	constexpr uint64_t P12 = static_cast<uint64_t>(C::p1) * C::p2;
 	const uint32_t x1m2 = (x[0] >= C::p2) ? x[0] - C::p2 : x[0];
-	const uint32_t a2 = Z2::mul(Z2::sub(x[1], x1m2), C::c12);
+	const uint32_t a2 = shoup_mul(Z2::sub(x[1], x1m2), C::s12, C::p2);
 	const uint32_t x1m3 = (x[0] >= C::p3) ? x[0] - C::p3 : x[0];
-	const uint32_t a3 = Z3::mul(Z3::sub(x[2], Z3::add(x1m3, Z3::mul(a2, C::p1m3))), C::c123);
+	const uint32_t a3 = shoup_mul(Z3::sub(x[2], Z3::add(x1m3, shoup_mul(a2, C::s1_3, C::p3))), C::s123, C::p3);
 	const uint64_t low = static_cast<uint64_t>(a2) * C::p1 + x[0];          // < p1 p2
 	const bool z = (a3 > (C::p3 - 1) / 2) || ((a3 == (C::p3 - 1) / 2) && (low > P12 / 2));
 	const uint64_t U = (low << dup) + static_cast<uint64_t>(K.r[dup]) * a3 + K.h + (z ? K.b - K.mr[dup] : 0u);
@@ -396,13 +405,12 @@ __device__ __forceinline__ void crt_garner4(uint32_t (&x)[4])
 	using Z4 = Zp<C::p4, true>;
 	const uint32_t a1 = x[0];
 	const uint32_t a1m2 = (a1 >= C::p2) ? a1 - C::p2 : a1;
-	const uint32_t a2 = Z2::mul(Z2::sub(x[1], a1m2), C::c12);
+	const uint32_t a2 = shoup_mul(Z2::sub(x[1], a1m2), C::s12, C::p2);
 	const uint32_t a1m3 = (a1 >= C::p3) ? a1 - C::p3 : a1;
-	const uint32_t a3 = Z3::mul(Z3::sub(x[2], Z3::add(a1m3, Z3::mul(a2, C::p1m3))), C::c123);
+	const uint32_t a3 = shoup_mul(Z3::sub(x[2], Z3::add(a1m3, shoup_mul(a2, C::s1_3, C::p3))), C::s123, C::p3);
 	const uint32_t a1m4 = (a1 >= C::p4) ? a1 - C::p4 : a1;
-	const uint32_t a2m4 = (a2 >= C::p4) ? a2 - C::p4 : a2;
-	const uint32_t s4 = Z4::add(Z4::add(a1m4, Z4::mul(a2m4, C::p1m4)), Z4::mul(a3, C::p12m4));
-	const uint32_t a4 = Z4::mul(Z4::sub(x[3], s4), C::c1234);
+	const uint32_t s4 = Z4::add(Z4::add(a1m4, shoup_mul(a2, C::s1_4, C::p4)), shoup_mul(a3, C::s12_4, C::p4));
+	const uint32_t a4 = shoup_mul(Z4::sub(x[3], s4), C::s1234, C::p4);
 	// V > M/2 by mixed-radix digits from the top (M/2 = T (p4 - 1)/2 + T/2, T = p1 p2 p3)
 	constexpr uint64_t P12 = static_cast<uint64_t>(C::p1) * C::p2;
 	const uint64_t low = static_cast<uint64_t>(a2) * C::p1 + a1;            // < p1 p2
