@@ -626,14 +626,20 @@ void row_t(const Args &a, int grid_y, cudaStream_t s, bool prep, int planes)
 	using S = RowShape<LC>;
 	const size_t smem = size_t(S::PC) * 4;          // one plane per CTA
 	if (prep) { set_smem(k_row<LC>, smem); set_smem(k_row2<LC>, 2 * smem); set_smem(k_rowp<LC>, 2 * smem); return; }
-	if ((planes == 4) && (a.op != OP_FWD) && a.twist)
+	// A pair per CTA halves the grid: it pays for rows of 8192 points (512
+	// threads, one CTA per SM) and from 1024 CTAs of single rows; below, the
+	// single rows run in parallel instead (two packed tests at n = 17, 128 row
+	// CTAs: 36.6 -> 22.5 us per squaring unpaired, four 42.4 -> 35.0; two at
+	// n = 18 with 8192-point rows 37.2 paired against 39.6).
+	const bool pair = (LC >= 13) || ((size_t(1) << (a.n - LC)) * 4 * size_t(grid_y) >= 1024);
+	if ((planes == 4) && (a.op != OP_FWD) && a.twist && pair)
 	{
 		// twisted packed rows share their roots: two rows of a test per CTA (k_rowp)
 		const dim3 grid((1u << (a.n - LC - 1)) * 4u, static_cast<unsigned>(grid_y));
 		launch_pdl(k_rowp<LC>, grid, dim3(row_threads(LC)), 2 * smem, s, a);
 		return;
 	}
-	if ((planes == 4) && (a.op != OP_FWD) && (grid_y >= 2))
+	if ((planes == 4) && (a.op != OP_FWD) && (grid_y >= 2) && pair)
 	{
 		// packed batches: two tests per CTA sharing the row's roots (k_row2)
 		const dim3 grid((1u << (a.n - LC)) * 4u, static_cast<unsigned>((grid_y + 1) / 2));
