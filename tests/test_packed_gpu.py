@@ -148,6 +148,34 @@ def test_twisted_packed_blocks_match_four_step(n, plan, ref, count):
         assert np.array_equal(canon(got[2][i], b), canon(want[2][i], b)), i
 
 
+@pytest.mark.parametrize("n,count", [(17, 2), (17, 4), (18, 2)])
+def test_small_packed_batches_match_unpacked(n, count):
+    """Packed batches of a few tests: at n = 17 their row CTAs run one test's row
+    each (a pair per CTA would halve a grid of 128-256 CTAs), at n = 18 (rows
+    of 8192 points) two tests' rows per CTA; Gerbicz-Li blocks against the
+    unpacked four-step plan."""
+    rng = np.random.default_rng(n * 10 + count)
+    bases = [int(x) & ~1 for x in rng.integers(1_100_000, 100_000_000, size=count)]
+    B = 20
+    exps = [gf.Job.prefix(b, n, 4 * B + (i % 5)).words_nbits() for i, b in enumerate(bases)]
+    got = _blocks(bases, n, 204, B, 2, exps)
+    want = _blocks(bases, n, 4 if n == 17 else 5, B, 2, exps)
+    assert np.array_equal(got[0], want[0])
+    for i, b in enumerate(bases):
+        assert np.array_equal(canon(got[1][i], b), canon(want[1][i], b)), i
+        assert np.array_equal(canon(got[2][i], b), canon(want[2][i], b)), i
+
+
+@pytest.mark.parametrize("n,count,plan", [(20, 1, 303), (20, 2, 304), (21, 1, 305), (21, 3, 304), (22, 1, 305),
+                                          (22, 2, 306), (23, 2, 306)])
+def test_packed_default_plans_by_count(n, count, plan):
+    """A new packed batch starts on the plan measured fastest for its size and
+    number of tests."""
+    bases = [20_000_002 + 2 * i for i in range(count)]
+    with Batch(bases, n) as bt:
+        assert bt.plan() == plan
+
+
 def test_plan_switch_with_pending_carries(oracle):
     """Carries left pending by one plan are absorbed before the next takes over."""
     n, b = 16, 60_000_002
