@@ -760,15 +760,18 @@ void cluster_t(const Args &a, int ntests, int max_active, cudaStream_t s, bool p
 	after_launch();
 }
 
-// Cluster shape by size: n = 12..14 on eight CTAs with rows of 2^(n-3)
-// (plane-split passes), n = 15..17 on 2..8 CTAs with rows of 2^13.
+// Cluster shape by size: n = 12..14 with plane-split passes on rows of
+// 2^(n-LQ) (eight CTAs at n = 12, 13 and 16 at n = 14), n = 15..17 on 2..16
+// CTAs with rows of 2^13.  On one B200 (graph replay, us per squaring), 8 ->
+// 16 CTAs: n = 14 12.94 -> 11.22 for one test, 13.12 -> 11.28 for four;
+// n = 12 9.66 -> 9.89 and 10.11 -> 9.90 (kept on eight); n = 13 10.41 -> 11.01.
 void launch_cluster_n(int n, const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
 {
 	switch (n)
 	{
 		case 12: cluster_t<3, 9>(a, ntests, max_active, s, prep, max_out); break;
 		case 13: cluster_t<3, 10>(a, ntests, max_active, s, prep, max_out); break;
-		case 14: cluster_t<3, 11>(a, ntests, max_active, s, prep, max_out); break;
+		case 14: cluster_t<4, 10>(a, ntests, max_active, s, prep, max_out); break;
 		case 15: cluster_t<2, 13>(a, ntests, max_active, s, prep, max_out); break;
 		case 16: cluster_t<3, 13>(a, ntests, max_active, s, prep, max_out); break;
 		case 17: cluster_t<4, 13>(a, ntests, max_active, s, prep, max_out); break;
