@@ -289,11 +289,15 @@ struct CarryK
 // f T top = (Q b + R) top folded into U < 2^64, so one 64-bit division by b
 // remains; the quotient is assembled modulo 2^64, which is exact because the
 // carry of a resting register is below 2^55 in magnitude.
+//
+// crt_split does everything that does not depend on c: u = U + K b and
+// t = Q top - z (mq + 1) - K (both modulo 2^64); crt_chain then adds the
+// carry, divides once and returns the digit.  crt_carry is the two in one.
 template <int SET>
-__device__ __forceinline__ int32_t crt_carry(const uint32_t x[3], int dup, const CarryK &K, int64_t &c);
+__device__ __forceinline__ void crt_split(const uint32_t x[3], int dup, const CarryK &K, uint64_t &u, uint64_t &t);
 
 template <>
-__device__ __forceinline__ int32_t crt_carry<0>(const uint32_t x[3], int dup, const CarryK &K, int64_t &c)
+__device__ __forceinline__ void crt_split<0>(const uint32_t x[3], int dup, const CarryK &K, uint64_t &u, uint64_t &t)
 {
 	using C = Crt<0>;
 	using Z2 = Zp<C::p2, false>;
@@ -301,15 +305,12 @@ __device__ __forceinline__ int32_t crt_carry<0>(const uint32_t x[3], int dup, co
 	const uint32_t x1m2 = (x[0] >= C::p2) ? x[0] - C::p2 : x[0];
 	const uint32_t a2 = Z2::mul(Z2::sub(x[1], x1m2), C::c12);
 	const bool z = (static_cast<uint64_t>(a2) * C::p1 + x[0]) > M / 2;
-	const uint64_t U = (static_cast<uint64_t>(x[0]) << dup) + static_cast<uint64_t>(K.r[dup]) * a2 + K.h + (z ? K.b - K.mr[dup] : 0u);
-	uint64_t rv;
-	const uint64_t qv = divb64(U + static_cast<uint64_t>(c) + K.kb, K.b, K.binv, rv);
-	c = static_cast<int64_t>(qv + K.q[dup] * a2 - (z ? K.mq[dup] + 1 : 0) - K.k);
-	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
+	u = (static_cast<uint64_t>(x[0]) << dup) + static_cast<uint64_t>(K.r[dup]) * a2 + K.h + (z ? K.b - K.mr[dup] : 0u) + K.kb;
+	t = K.q[dup] * a2 - (z ? K.mq[dup] + 1 : 0) - K.k;
 }
 
 template <>
-__device__ __forceinline__ int32_t crt_carry<1>(const uint32_t x[3], int dup, const CarryK &K, int64_t &c)
+__device__ __forceinline__ void crt_split<1>(const uint32_t x[3], int dup, const CarryK &K, uint64_t &u, uint64_t &t)
 {
 	using C = Crt<1>;
 	using Z2 = Zp<C::p2, true>;
@@ -321,11 +322,24 @@ __device__ __forceinline__ int32_t crt_carry<1>(const uint32_t x[3], int dup, co
 	const uint32_t a3 = shoup_mul(Z3::sub(x[2], Z3::add(x1m3, shoup_mul(a2, C::s1_3, C::p3))), C::s123, C::p3);
 	const uint64_t low = static_cast<uint64_t>(a2) * C::p1 + x[0];          // < p1 p2
 	const bool z = (a3 > (C::p3 - 1) / 2) || ((a3 == (C::p3 - 1) / 2) && (low > P12 / 2));
-	const uint64_t U = (low << dup) + static_cast<uint64_t>(K.r[dup]) * a3 + K.h + (z ? K.b - K.mr[dup] : 0u);
+	u = (low << dup) + static_cast<uint64_t>(K.r[dup]) * a3 + K.h + (z ? K.b - K.mr[dup] : 0u) + K.kb;
+	t = K.q[dup] * a3 - (z ? K.mq[dup] + 1 : 0) - K.k;
+}
+
+__device__ __forceinline__ int32_t crt_chain(uint64_t u, uint64_t t, const CarryK &K, int64_t &c)
+{
 	uint64_t rv;
-	const uint64_t qv = divb64(U + static_cast<uint64_t>(c) + K.kb, K.b, K.binv, rv);
-	c = static_cast<int64_t>(qv + K.q[dup] * a3 - (z ? K.mq[dup] + 1 : 0) - K.k);
+	const uint64_t qv = divb64(u + static_cast<uint64_t>(c), K.b, K.binv, rv);
+	c = static_cast<int64_t>(qv + t);
 	return static_cast<int32_t>(rv) - static_cast<int32_t>(K.h);
+}
+
+template <int SET>
+__device__ __forceinline__ int32_t crt_carry(const uint32_t x[3], int dup, const CarryK &K, int64_t &c)
+{
+	uint64_t u, t;
+	crt_split<SET>(x, dup, K, u, t);
+	return crt_chain(u, t, K, c);
 }
 
 // Balanced digit of s (|s| < 2^62) and carry floor((s + b/2) / b).

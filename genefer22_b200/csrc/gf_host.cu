@@ -761,16 +761,17 @@ void cluster_t(const Args &a, int ntests, int max_active, cudaStream_t s, bool p
 }
 
 // Cluster shape by size: n = 12..14 with plane-split passes on rows of
-// 2^(n-LQ) (eight CTAs at n = 12, 13 and 16 at n = 14), n = 15..17 on 2..16
-// CTAs with rows of 2^13.  On one B200 (graph replay, us per squaring), 8 ->
-// 16 CTAs: n = 14 12.94 -> 11.22 for one test, 13.12 -> 11.28 for four;
-// n = 12 9.66 -> 9.89 and 10.11 -> 9.90 (kept on eight); n = 13 10.41 -> 11.01.
+// 2^(n-LQ) (eight CTAs at n = 12, 16 at n = 13, 14), n = 15..17 on 2..16 CTAs
+// with rows of 2^13.  One test on one B200 (graph replay, us per squaring),
+// 8 -> 16 CTAs with the balanced row schedule: n = 12 6.75 -> 9.95 (2^8-point
+// rows of two 16-point passes leave half of the threads idle), n = 13 8.80 ->
+// 8.31; n = 14 13.04 (eight CTAs, earlier schedule) -> 10.40.
 void launch_cluster_n(int n, const Args &a, int ntests, int max_active, cudaStream_t s, bool prep, int *max_out)
 {
 	switch (n)
 	{
 		case 12: cluster_t<3, 9>(a, ntests, max_active, s, prep, max_out); break;
-		case 13: cluster_t<3, 10>(a, ntests, max_active, s, prep, max_out); break;
+		case 13: cluster_t<4, 9>(a, ntests, max_active, s, prep, max_out); break;
 		case 14: cluster_t<4, 10>(a, ntests, max_active, s, prep, max_out); break;
 		case 15: cluster_t<2, 13>(a, ntests, max_active, s, prep, max_out); break;
 		case 16: cluster_t<3, 13>(a, ntests, max_active, s, prep, max_out); break;

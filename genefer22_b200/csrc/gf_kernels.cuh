@@ -231,6 +231,19 @@ struct Sched
 {
 	static constexpr int NP = (L + 3) / 4;
 	__host__ __device__ static constexpr int r(int p) { return (p < L / 4) ? 4 : (L % 4); }
+	__host__ __device__ static constexpr int s(int p) { return 4 * p; }
+};
+
+// Balanced schedule: as few passes as Sched, their radices differing by one at
+// most, the larger ones last (2^9: 3, 3, 3; 2^10: 3, 3, 4; 2^11: 3, 4, 4), so
+// that the groups of every pass but the last are 8 points.
+template <int L>
+struct SchedB
+{
+	static constexpr int NP = (L + 3) / 4;
+	static constexpr int LO = L / NP, HI = NP - L % NP;   // passes p >= HI take LO + 1 stages
+	__host__ __device__ static constexpr int r(int p) { return LO + ((p >= HI) ? 1 : 0); }
+	__host__ __device__ static constexpr int s(int p) { return LO * p + ((p > HI) ? p - HI : 0); }
 };
 
 // ------------------------------------------------------------------ passes
@@ -325,32 +338,33 @@ __device__ __forceinline__ void pass_all(uint32_t *buf, int pstride, int lanes_l
 	}
 }
 
-// Forward passes 0 .. NP-1 (or NP-2 with SKIP_LAST), a barrier after each.
-template <int SET, int L, bool SKIP_LAST, class Map, bool PSPLIT = false>
+// Forward passes 0 .. NP-1 (or NP-2 with SKIP_LAST) of schedule SC, a barrier
+// after each.
+template <int SET, int L, bool SKIP_LAST, class Map, bool PSPLIT = false, class SC = Sched<L>>
 __device__ __forceinline__ void run_fwd(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										uint32_t base_step, const Tables &tab, int pl_lo = 0, int pl_hi = PrimeSet<SET>::W)
 {
-	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
+	constexpr int NP = SC::NP - (SKIP_LAST ? 1 : 0);
 	static_for<0, NP>([&](auto P) {
 		constexpr int p = decltype(P)::value;
-		pass_all<SET, Sched<L>::r(p), PM_FWD, L, 4 * p, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, lane_fast, base0,
-																			   base_step, tab, nullptr, 0, nullptr, 0,
-																			   pl_lo, pl_hi);
+		pass_all<SET, SC::r(p), PM_FWD, L, SC::s(p), Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, lane_fast, base0,
+																			base_step, tab, nullptr, 0, nullptr, 0,
+																			pl_lo, pl_hi);
 		__syncthreads();
 	});
 }
 
 // Inverse passes NP-1 (or NP-2 with SKIP_LAST) .. 0.
-template <int SET, int L, bool SKIP_LAST, class Map, bool PSPLIT = false>
+template <int SET, int L, bool SKIP_LAST, class Map, bool PSPLIT = false, class SC = Sched<L>>
 __device__ __forceinline__ void run_inv(uint32_t *buf, int pstride, int lanes_log, bool lane_fast, uint32_t base0,
 										uint32_t base_step, const Tables &tab, int pl_lo = 0, int pl_hi = PrimeSet<SET>::W)
 {
-	constexpr int NP = Sched<L>::NP - (SKIP_LAST ? 1 : 0);
+	constexpr int NP = SC::NP - (SKIP_LAST ? 1 : 0);
 	static_for<0, NP>([&](auto Q) {
 		constexpr int p = NP - 1 - decltype(Q)::value;
-		pass_all<SET, Sched<L>::r(p), PM_INV, L, 4 * p, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, lane_fast, base0,
-																			   base_step, tab, nullptr, 0, nullptr, 0,
-																			   pl_lo, pl_hi);
+		pass_all<SET, SC::r(p), PM_INV, L, SC::s(p), Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, lane_fast, base0,
+																			base_step, tab, nullptr, 0, nullptr, 0,
+																			pl_lo, pl_hi);
 		__syncthreads();
 	});
 }
@@ -507,21 +521,21 @@ __device__ __forceinline__ void row_core_pair(uint32_t *buf0, uint32_t *buf1, ui
 
 // Row transforms in shared memory: forward (OP_FWD), or forward + pointwise
 // square / product + inverse.
-template <int SET, int L, class Map, bool PSPLIT = false>
+template <int SET, int L, class Map, bool PSPLIT = false, class SC = Sched<L>>
 __device__ __forceinline__ void row_core(uint32_t *buf, int pstride, int lanes_log, uint32_t base0, const Tables &tab,
 										 const uint32_t *zrow, size_t zstride, int op)
 {
-	constexpr int PL = Sched<L>::NP - 1;
-	if (op == OP_FWD) { run_fwd<SET, L, false, Map, PSPLIT>(buf, pstride, lanes_log, false, base0, 1u, tab); return; }
-	run_fwd<SET, L, true, Map, PSPLIT>(buf, pstride, lanes_log, false, base0, 1u, tab);
+	constexpr int PL = SC::NP - 1;
+	if (op == OP_FWD) { run_fwd<SET, L, false, Map, PSPLIT, SC>(buf, pstride, lanes_log, false, base0, 1u, tab); return; }
+	run_fwd<SET, L, true, Map, PSPLIT, SC>(buf, pstride, lanes_log, false, base0, 1u, tab);
 	if (op == OP_MUL)
-		pass_all<SET, Sched<L>::r(PL), PM_MID_MUL, L, 4 * PL, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, false, base0,
-																					  1u, tab, zrow, zstride);
+		pass_all<SET, SC::r(PL), PM_MID_MUL, L, SC::s(PL), Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, false, base0,
+																				  1u, tab, zrow, zstride);
 	else
-		pass_all<SET, Sched<L>::r(PL), PM_MID_SQ, L, 4 * PL, Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, false, base0,
-																					 1u, tab, zrow, zstride);
+		pass_all<SET, SC::r(PL), PM_MID_SQ, L, SC::s(PL), Map, IO_SMEM, PSPLIT>(buf, pstride, lanes_log, false, base0,
+																				 1u, tab, zrow, zstride);
 	__syncthreads();
-	run_inv<SET, L, true, Map, PSPLIT>(buf, pstride, lanes_log, false, base0, 1u, tab);
+	run_inv<SET, L, true, Map, PSPLIT, SC>(buf, pstride, lanes_log, false, base0, 1u, tab);
 }
 
 // ------------------------------------------------------------------ k_small
@@ -661,10 +675,11 @@ __global__ void __launch_bounds__(SmallShape<SET, LOGN, SPLIT>::T, SmallShape<SE
 // clusters takes tests t = cluster, cluster + clusters, ...
 //
 // Rows of 2^13 (n = 15..17, LQ = 2..4) have one owner thread per segment and
-// no more threads.  Shorter rows (n = 12..14 on eight CTAs, LC = 9..11) add
-// plane-split threads: the transform passes and column transforms run a thread
-// per (plane, group), three times the owners, so that a lone small test spread
-// over eight SMs still keeps several warps on each.
+// no more threads.  Shorter rows (n = 12..14, LC = 9..11) add plane-split
+// threads: the transform passes (balanced schedule, 8-point groups) and column
+// transforms run a thread per (plane, group), W C / 8 threads, so that a lone
+// small test spread over 8 or 16 SMs keeps several warps on each and a thread
+// takes one group per pass.
 template <int LQ, int LC = 13>
 struct ClusterShape
 {
@@ -678,9 +693,12 @@ struct ClusterShape
 	// b >= 1024, absorb() checks it)
 	static constexpr int D = PS ? SEG / 2 : SEG;
 	static constexpr int T0 = C / D;                      // owner threads
-	static constexpr int T = PS ? ((WMAX * C / SEG > T0) ? WMAX * C / SEG : T0) : T0;
+	static constexpr int T = PS ? WMAX * C / 8 : T0;
 	static constexpr int MINB = PS ? 1 : 2;
-	static constexpr size_t SMEM = size_t(WMAX) * PC * 4 + size_t(T0) * 8;
+	// planes, the owners' carries, and (PS) a fourth word per digit for the
+	// two-stage CRT
+	static constexpr size_t SMEM = size_t(WMAX) * PC * 4 + size_t(T0) * 8 + (PS ? size_t(PC) * 4 : 0);
+	using SC = std::conditional_t<PS, SchedB<LC>, Sched<LC>>;
 	static_assert(T <= 1024, "threads per CTA");
 };
 
@@ -809,11 +827,47 @@ __device__ __forceinline__ void cluster_test(const Args &a, int t, const TestDes
 		cl.sync();
 		cluster_cols<SET, LQ, LC, false>(sm, q, tab);
 		cl.sync();
-		row_core<SET, LC, MP, S::PS>(sm, PC, 0, (1u << LQ) + static_cast<uint32_t>(q), tab, nullptr, 0, OP_SQUARE);
+		row_core<SET, LC, MP, S::PS, typename S::SC>(sm, PC, 0, (1u << LQ) + static_cast<uint32_t>(q), tab, nullptr, 0,
+													  OP_SQUARE);
 		cl.sync();
 		cluster_cols<SET, LQ, LC, true>(sm, q, tab);
 		cl.sync();
-		if (owner)
+		if constexpr (S::PS)
+		{
+			// every thread takes digits j = tid, tid + T, ... through the part of
+			// the CRT that needs no carry and leaves (u, t) in the digit's plane
+			// words and ex; the owners then run their carry chains alone
+			uint32_t *const ex = reinterpret_cast<uint32_t *>(sc + T0);
+#pragma unroll 1
+			for (int j = tid; j < C; j += S::T)
+			{
+				const int aj = MP::addr(j, 0);
+				uint32_t x[3];
+#pragma unroll
+				for (int pl = 0; pl < W; ++pl) x[pl] = sm[pl * PC + aj];
+				uint64_t u, tt;
+				crt_split<SET>(x, dup ? 1 : 0, d.ck, u, tt);
+				sm[aj] = static_cast<uint32_t>(u);
+				sm[PC + aj] = static_cast<uint32_t>(u >> 32);
+				sm[2 * PC + aj] = static_cast<uint32_t>(tt);
+				ex[aj] = static_cast<uint32_t>(tt >> 32);
+			}
+			__syncthreads();
+			if (owner)
+			{
+				int64_t c = 0;
+#pragma unroll
+				for (int i = 0; i < D; ++i)
+				{
+					const int aj = MP::addr(tid * D + i, 0);
+					const uint64_t u = sm[aj] | (static_cast<uint64_t>(sm[PC + aj]) << 32);
+					const uint64_t tt = sm[2 * PC + aj] | (static_cast<uint64_t>(ex[aj]) << 32);
+					dg[i] = crt_chain(u, tt, d.ck, c);
+				}
+				sc[tid] = c;
+			}
+		}
+		else if (owner)
 		{
 			int64_t c = 0;
 #pragma unroll
