@@ -246,6 +246,23 @@ struct SchedB
 	__host__ __device__ static constexpr int s(int p) { return LO * p + ((p > HI) ? p - HI : 0); }
 };
 
+// Every pass of a schedule starts where the one before it ends, and the
+// passes cover the L stages.
+template <class SC, int L>
+constexpr bool sched_covers()
+{
+	int at = 0;
+	for (int p = 0; p < SC::NP; ++p)
+	{
+		if ((SC::s(p) != at) || (SC::r(p) < 1) || (SC::r(p) > 4)) return false;
+		at += SC::r(p);
+	}
+	return at == L;
+}
+static_assert(sched_covers<SchedB<8>, 8>() && sched_covers<SchedB<9>, 9>() && sched_covers<SchedB<10>, 10>() &&
+				  sched_covers<SchedB<11>, 11>() && sched_covers<SchedB<13>, 13>(),
+			  "balanced radix schedule");
+
 // ------------------------------------------------------------------ passes
 
 // One radix-2^r pass over the W planes (pstride words apart) of a shared-memory
