@@ -2,8 +2,8 @@
 
 A plan is the split of the length-N transform: ``lr = 0`` keeps a whole test
 in one CTA's shared memory (n <= 14); ``lr = 1`` keeps it in the shared
-memory of a thread-block cluster (eight CTAs for 12 <= n <= 14, 2^(n-13) CTAs
-for 15 <= n <= 17); ``100 +
+memory of a thread-block cluster (eight CTAs at n = 12, sixteen at n = 13, 14,
+2^(n-13) CTAs for 15 <= n <= 17); ``100 +
 lr2`` splits the column transform into a 16-point register pass and a
 2^lr2-point middle pass (six-step); ``200 + lr`` (four-step) and ``300 + lr2`` (six-step)
 pack two base-b digits into one coefficient of a half-length transform over

@@ -839,9 +839,10 @@ constexpr int PLAN_PACKED_SIX = 300;   // plan codes 300 + lr2: packed digits, s
 
 constexpr int PLAN_CLUSTER = 1;   // plan code of the cluster-resident squaring
 // A batch of at most this many tests of size 12..14 squares on the cluster
-// plan by default: one test on eight SMs instead of one (a lone n = 12, 13,
-// 14 test 15.4 -> 12.0, 31.3 -> 11.9, 62.4 -> 14.9 us per squaring, graph
-// replay on one B200); larger batches fill the SMs with one CTA per test.
+// plan by default: one test on 8 or 16 SMs instead of one (a lone n = 12, 13,
+// 14 test on one CTA 15.4, 31.3, 62.4 us per squaring; on the cluster now
+// 6.6, 8.2, 10.3, graph replay on one B200); larger batches fill the SMs with
+// one CTA per test.
 constexpr size_t CLUSTER_MAX_TESTS = 4;
 
 bool plan_valid(int n, int lr)

@@ -207,8 +207,8 @@ int gfc_batch_set_all(gfc_batch *bt, size_t reg, const int32_t *in);
 /* Kernel plan.  lr = 0: one CTA per test with the state in shared memory
  * (n <= 14); lr = 1: squarings by one thread-block cluster per test with the
  * state in the cluster's shared memory (12 <= n <= 17: eight CTAs with rows of
- * 2^(n-3) up to n = 14, 2^(n-13) CTAs with rows of 2^13 above; products use the
- * default plan of n); 3 <= lr <= 10: four-step with R = 2^lr rows
+ * 2^9 at n = 12, sixteen with rows of 2^(n-4) at n = 13, 14, 2^(n-13) CTAs with
+ * rows of 2^13 above; products use the default plan of n); 3 <= lr <= 10: four-step with R = 2^lr rows
  * (8 <= n - lr <= 13); lr = 100 + lr2 (3 <= lr2 <= 7): six-step, the column
  * transform split into 2^4 and 2^lr2 points (8 <= n - 4 - lr2 <= 13);
  * lr = 200 + l (l = 3, 4): packed digits, two base-b digits per coefficient
